@@ -1,0 +1,229 @@
+// C ABI, layer 1: the reference's own C signatures with host pointers.
+//
+// Each call stages its inputs into device memory drawn from the stream-ordered
+// pool of the calling thread's per-thread default stream, runs the device
+// entry point and copies the results back before it returns.  Calls made from
+// different host threads use different streams and do not share buffers.
+#include <string.h>
+
+#include "common.cuh"
+
+static thread_local int t_last_status = ID11B_OK;
+static thread_local int t_last_cuda = 0;
+
+int id11b_record_cuda(cudaError_t e) {
+    t_last_cuda = (int)e;
+    return ID11B_ERR_CUDA;
+}
+
+extern "C" int id11b_version(void) { return 100; }
+
+extern "C" const char* id11b_status_string(int status) {
+    switch (status) {
+        case ID11B_OK: return "ok";
+        case ID11B_ERR_ARG: return "invalid argument";
+        case ID11B_ERR_CUDA: return "CUDA error";
+        case ID11B_ERR_ALIGN: return "misaligned pointer";
+        case ID11B_ERR_SIZE: return "size beyond the supported maximum";
+        case ID11B_ERR_TIMEOUT: return "bounded device wait timed out";
+        case ID11B_ERR_NODEV: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+extern "C" int id11b_last_cuda_error(void) { return t_last_cuda; }
+extern "C" int id11b_last_status(void) { return t_last_status; }
+
+namespace {
+
+// One pooled device allocation for the whole call, freed in stream order.
+struct Staging {
+    cudaStream_t st = cudaStreamPerThread;
+    char* base = nullptr;
+    size_t used = 0, cap = 0;
+    int status = ID11B_OK;
+    explicit Staging(size_t bytes) {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+            cudaGetLastError();
+            status = ID11B_ERR_NODEV;
+            return;
+        }
+        cap = bytes + 256 * 8;
+        cudaError_t e = cudaMallocAsync((void**)&base, cap, st);
+        if (e != cudaSuccess) status = id11b_record_cuda(e);
+    }
+    ~Staging() {
+        if (base) cudaFreeAsync(base, st);
+    }
+    template <class T>
+    T* take(size_t count) {
+        size_t off = (used + 255) & ~(size_t)255;
+        used = off + count * sizeof(T);
+        return reinterpret_cast<T*>(base + off);
+    }
+    int h2d(void* d, const void* h, size_t bytes) {
+        if (status || !bytes) return status;
+        cudaError_t e = cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) status = id11b_record_cuda(e);
+        return status;
+    }
+    int d2h(void* h, const void* d, size_t bytes) {
+        if (status || !bytes) return status;
+        cudaError_t e = cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) status = id11b_record_cuda(e);
+        return status;
+    }
+    int run(int rc) {
+        if (!status && rc) status = rc;
+        return status;
+    }
+    int sync() {
+        if (status) return status;
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) status = id11b_record_cuda(e);
+        return status;
+    }
+};
+
+int finish(Staging& s) {
+    s.sync();
+    t_last_status = s.status;
+    return s.status;
+}
+
+}  // namespace
+
+extern "C" void id11b_compute_gv(double xlylzl[][3], double omega[], double omegasign,
+                                 double wvln, double wedge, double chi, double t[3],
+                                 double gv[][3], int n) {
+    if (n < 0) { t_last_status = ID11B_ERR_ARG; return; }
+    Staging s(sizeof(double) * (size_t)n * 7);
+    double* dx = s.take<double>(3 * (size_t)n);
+    double* dom = s.take<double>(n);
+    double* dg = s.take<double>(3 * (size_t)n);
+    s.h2d(dx, xlylzl, sizeof(double) * 3 * (size_t)n);
+    s.h2d(dom, omega, sizeof(double) * (size_t)n);
+    if (!s.status)
+        s.run(id11b_dev_compute_gv(dx, dom, omegasign, wvln, wedge, chi, t, dg, nullptr, n, s.st));
+    s.d2h(gv, dg, sizeof(double) * 3 * (size_t)n);
+    finish(s);
+}
+
+extern "C" void id11b_compute_geometry(double xlylzl[][3], double omega[], double omegasign,
+                                       double wvln, double wedge, double chi, double t[3],
+                                       double out[][6], int n) {
+    if (n < 0) { t_last_status = ID11B_ERR_ARG; return; }
+    Staging s(sizeof(double) * (size_t)n * 10);
+    double* dx = s.take<double>(3 * (size_t)n);
+    double* dom = s.take<double>(n);
+    double* dout = s.take<double>(6 * (size_t)n);
+    s.h2d(dx, xlylzl, sizeof(double) * 3 * (size_t)n);
+    s.h2d(dom, omega, sizeof(double) * (size_t)n);
+    if (!s.status)
+        s.run(id11b_dev_compute_geometry(dx, dom, omegasign, wvln, wedge, chi, t, dout, n, s.st));
+    s.d2h(out, dout, sizeof(double) * 6 * (size_t)n);
+    finish(s);
+}
+
+extern "C" void id11b_compute_xlylzl(double sl[], double f[], double p[4], double r[9],
+                                     double dist[3], double xlylzl[][3], int n) {
+    if (n < 0) { t_last_status = ID11B_ERR_ARG; return; }
+    Staging s(sizeof(double) * (size_t)n * 5);
+    double* ds = s.take<double>(n);
+    double* df = s.take<double>(n);
+    double* dx = s.take<double>(3 * (size_t)n);
+    s.h2d(ds, sl, sizeof(double) * (size_t)n);
+    s.h2d(df, f, sizeof(double) * (size_t)n);
+    if (!s.status) s.run(id11b_dev_compute_xlylzl(ds, df, p, r, dist, dx, n, s.st));
+    s.d2h(xlylzl, dx, sizeof(double) * 3 * (size_t)n);
+    finish(s);
+}
+
+extern "C" int id11b_score(double ubi[3][3], double gv[][3], double tol, int ng) {
+    if (ng < 0) { t_last_status = ID11B_ERR_ARG; return -1; }
+    Staging s(sizeof(double) * (3 * (size_t)ng + 9) + 64);
+    double* du = s.take<double>(9);
+    double* dg = s.take<double>(3 * (size_t)ng);
+    int32_t* dc = s.take<int32_t>(1);
+    int32_t count = -1;
+    s.h2d(du, ubi, sizeof(double) * 9);
+    s.h2d(dg, gv, sizeof(double) * 3 * (size_t)ng);
+    if (!s.status) s.run(id11b_dev_score(du, dg, tol, ng, dc, s.st));
+    s.d2h(&count, dc, sizeof(int32_t));
+    return finish(s) ? -1 : count;
+}
+
+static void lsq_host(int mode, double ubi[3][3], double gv[][3], double tol, int labels[],
+                     int label, int* n_out, double* mean_out, int ng) {
+    if (ng < 0) { t_last_status = ID11B_ERR_ARG; return; }
+    int64_t wsb = id11b_lsq_workspace_bytes(ng);
+    Staging s(sizeof(double) * (3 * (size_t)ng + 9) + sizeof(int) * (size_t)(mode ? ng : 0) +
+              (size_t)wsb + 64);
+    double* du = s.take<double>(9);
+    double* dg = s.take<double>(3 * (size_t)ng);
+    int32_t* dl = mode ? s.take<int32_t>(ng) : nullptr;
+    char* ws = s.take<char>(wsb);
+    int32_t* dn = s.take<int32_t>(1);
+    double* dm = s.take<double>(1);
+    s.h2d(du, ubi, sizeof(double) * 9);
+    s.h2d(dg, gv, sizeof(double) * 3 * (size_t)ng);
+    if (mode) s.h2d(dl, labels, sizeof(int32_t) * (size_t)ng);
+    if (!s.status) {
+        if (mode == 0)
+            s.run(id11b_dev_score_and_refine(du, dg, tol, ng, dn, dm, ws, wsb, s.st));
+        else
+            s.run(id11b_dev_refine_assigned(du, dg, dl, label, ng, dn, dm, ws, wsb, s.st));
+    }
+    int32_t n = 0;
+    double mean = 0.;
+    double u[9];
+    s.d2h(u, du, sizeof(u));
+    s.d2h(&n, dn, sizeof(n));
+    s.d2h(&mean, dm, sizeof(mean));
+    if (finish(s) == ID11B_OK) {
+        memcpy(ubi, u, sizeof(u));
+        *n_out = n;
+        *mean_out = mean;
+    }
+}
+
+extern "C" void id11b_score_and_refine(double ubi[3][3], double gv[][3], double tol,
+                                       int* n_arg, double* sumdrlv2_arg, int ng) {
+    lsq_host(0, ubi, gv, tol, nullptr, 0, n_arg, sumdrlv2_arg, ng);
+}
+
+extern "C" void id11b_refine_assigned(double ubi[3][3], double gv[][3], int labels[],
+                                      int label, int* npk, double* sumdrlv2, int ng) {
+    lsq_host(1, ubi, gv, 0., labels, label, npk, sumdrlv2, ng);
+}
+
+extern "C" int id11b_score_and_assign(double ubi[3][3], double gv[][3], double tol,
+                                      double drlv2[], int labels[], int label, int ng) {
+    if (ng < 0) { t_last_status = ID11B_ERR_ARG; return -1; }
+    Staging s(sizeof(double) * (4 * (size_t)ng + 9) + sizeof(int) * (size_t)ng + 64);
+    double* du = s.take<double>(9);
+    double* dg = s.take<double>(3 * (size_t)ng);
+    double* dd = s.take<double>(ng);
+    int32_t* dl = s.take<int32_t>(ng);
+    int32_t* dc = s.take<int32_t>(1);
+    s.h2d(du, ubi, sizeof(double) * 9);
+    s.h2d(dg, gv, sizeof(double) * 3 * (size_t)ng);
+    s.h2d(dd, drlv2, sizeof(double) * (size_t)ng);
+    s.h2d(dl, labels, sizeof(int32_t) * (size_t)ng);
+    if (!s.status) s.run(id11b_dev_score_and_assign(du, dg, tol, dd, dl, label, ng, dc, s.st));
+    int32_t count = -1;
+    s.d2h(drlv2, dd, sizeof(double) * (size_t)ng);
+    s.d2h(labels, dl, sizeof(int32_t) * (size_t)ng);
+    s.d2h(&count, dc, sizeof(int32_t));
+    return finish(s) ? -1 : count;
+}
+
+extern "C" int id11b_verify_rounding(int n) {
+    Staging s(64);
+    int32_t* db = s.take<int32_t>(1);
+    if (!s.status) s.run(id11b_dev_verify_rounding(n, db, s.st));
+    int32_t bad = -1;
+    s.d2h(&bad, db, sizeof(int32_t));
+    return finish(s) ? -1 : bad;
+}

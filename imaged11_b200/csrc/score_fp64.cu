@@ -1,0 +1,382 @@
+// Exact FP64 scoring kernels: the reference's arithmetic on the GPU.
+//
+// score, score_and_refine, refine_assigned, score_and_assign and
+// verify_rounding, one UBI per call, bit-exact in every decision with
+// ImageD11 src/closest.c (no FMA, left-to-right sums, magic-constant
+// rounding, strict drlv2 < tol^2).  Least-squares sums are reduced in a fixed
+// tree (per-thread partials -> warp butterfly -> CTA -> one finishing CTA), so
+// a call is reproducible run to run; the refined UBI differs from the
+// reference's sequential sum only by the rounding of that order (<1e-12
+// relative on the test sets).
+//
+// Also the plain batched FP64 scorer (many UBIs x many g, one launch per
+// tolerance set), the baseline against which the batched FP32 kernels are
+// measured.
+#include "common.cuh"
+
+namespace id11b {
+
+constexpr int kThreads = 256;
+constexpr int kLsqMaxBlocks = 1024;
+
+struct LsqPartial {
+    double r[9];   // sum ih_j * g_i       (R, row-major)
+    double h[6];   // sum ih_i * ih_j      (H upper triangle: 00 01 02 11 12 22)
+    double ss;     // sum drlv2
+    long long n;   // accepted peaks
+};
+
+__device__ __forceinline__ void load_ubi(const double* __restrict__ p, double u[9]) {
+#pragma unroll
+    for (int i = 0; i < 9; i++) u[i] = __ldg(p + i);
+}
+
+// ---------------------------------------------------------------- score ----
+__global__ void __launch_bounds__(kThreads)
+k_score(const double* __restrict__ ubi, const double* __restrict__ gv, double tolsq,
+        int64_t ng, int* __restrict__ count) {
+    double u[9];
+    load_ubi(ubi, u);
+    int n = 0;
+    for (int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x; k < ng;
+         k += (int64_t)gridDim.x * kThreads) {
+        double ih[3];
+        double s = drlv2_exact(u, __ldg(gv + 3 * k), __ldg(gv + 3 * k + 1),
+                               __ldg(gv + 3 * k + 2), ih);
+        n += (s < tolsq);
+    }
+    n = warp_sum(n);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(count, n);
+}
+
+// ------------------------------------------------------ LSQ (two stages) ----
+// Stage 1: per-CTA partial sums.  MODE 0 = score_and_refine (accept by tol),
+// MODE 1 = refine_assigned (accept by label).
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+k_lsq_partials(const double* __restrict__ ubi, const double* __restrict__ gv, double tolsq,
+               const int* __restrict__ labels, int label, int64_t ng,
+               LsqPartial* __restrict__ part) {
+    double u[9];
+    load_ubi(ubi, u);
+    double r[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double h[6] = {0, 0, 0, 0, 0, 0};
+    double ss = 0.;
+    long long n = 0;
+    for (int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x; k < ng;
+         k += (int64_t)gridDim.x * kThreads) {
+        if (MODE == 1 && __ldg(labels + k) != label) continue;
+        double g0 = __ldg(gv + 3 * k), g1 = __ldg(gv + 3 * k + 1), g2 = __ldg(gv + 3 * k + 2);
+        double ih[3];
+        double s = drlv2_exact(u, g0, g1, g2, ih);
+        if (MODE == 0 && !(s < tolsq)) continue;
+        n++;
+        ss = dadd(ss, s);
+        const double g[3] = {g0, g1, g2};
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) r[3 * i + j] = dadd(r[3 * i + j], dmul(ih[j], g[i]));
+        h[0] = dadd(h[0], dmul(ih[0], ih[0]));
+        h[1] = dadd(h[1], dmul(ih[1], ih[0]));
+        h[2] = dadd(h[2], dmul(ih[2], ih[0]));
+        h[3] = dadd(h[3], dmul(ih[1], ih[1]));
+        h[4] = dadd(h[4], dmul(ih[2], ih[1]));
+        h[5] = dadd(h[5], dmul(ih[2], ih[2]));
+    }
+    // warp butterfly, then CTA in warp order
+#pragma unroll
+    for (int i = 0; i < 9; i++) r[i] = warp_sum(r[i]);
+#pragma unroll
+    for (int i = 0; i < 6; i++) h[i] = warp_sum(h[i]);
+    ss = warp_sum(ss);
+    n = warp_sum(n);
+    __shared__ LsqPartial s_w[kThreads / 32];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int i = 0; i < 9; i++) s_w[w].r[i] = r[i];
+#pragma unroll
+        for (int i = 0; i < 6; i++) s_w[w].h[i] = h[i];
+        s_w[w].ss = ss;
+        s_w[w].n = n;
+    }
+    __syncthreads();
+    if (threadIdx.x < 17) {
+        const int f = threadIdx.x;
+        if (f < 16) {
+            double acc = 0.;
+            for (int q = 0; q < kThreads / 32; q++) {
+                const double* src = f < 9 ? s_w[q].r + f : (f < 15 ? s_w[q].h + (f - 9) : &s_w[q].ss);
+                acc += *src;
+            }
+            double* dst = f < 9 ? part[blockIdx.x].r + f
+                                : (f < 15 ? part[blockIdx.x].h + (f - 9) : &part[blockIdx.x].ss);
+            *dst = acc;
+        } else {
+            long long acc = 0;
+            for (int q = 0; q < kThreads / 32; q++) acc += s_w[q].n;
+            part[blockIdx.x].n = acc;
+        }
+    }
+}
+
+// Stage 2: one CTA sums the partials in a fixed order and applies the
+// reference's least-squares update (ImageD11 src/closest.c:326-344).
+__global__ void __launch_bounds__(kThreads)
+k_lsq_finish(const LsqPartial* __restrict__ part, int nparts, double* __restrict__ ubi,
+             int* __restrict__ n_out, double* __restrict__ mean_out) {
+    __shared__ double s_acc[kThreads / 32][16];
+    __shared__ long long s_n[kThreads / 32];
+    double acc[16];
+    long long n = 0;
+#pragma unroll
+    for (int f = 0; f < 16; f++) acc[f] = 0.;
+    for (int p = threadIdx.x; p < nparts; p += kThreads) {
+#pragma unroll
+        for (int i = 0; i < 9; i++) acc[i] += part[p].r[i];
+#pragma unroll
+        for (int i = 0; i < 6; i++) acc[9 + i] += part[p].h[i];
+        acc[15] += part[p].ss;
+        n += part[p].n;
+    }
+#pragma unroll
+    for (int f = 0; f < 16; f++) acc[f] = warp_sum(acc[f]);
+    n = warp_sum(n);
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int f = 0; f < 16; f++) s_acc[w][f] = acc[f];
+        s_n[w] = n;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t[16];
+        long long nn = 0;
+        for (int f = 0; f < 16; f++) t[f] = 0.;
+        for (int q = 0; q < kThreads / 32; q++) {
+            for (int f = 0; f < 16; f++) t[f] += s_acc[q][f];
+            nn += s_n[q];
+        }
+        double R[9], H[9];
+        for (int i = 0; i < 9; i++) R[i] = t[i];
+        H[0] = t[9];  H[1] = t[10]; H[2] = t[11];
+        H[3] = t[10]; H[4] = t[12]; H[5] = t[13];
+        H[6] = t[11]; H[7] = t[13]; H[8] = t[14];
+        double u[9];
+        for (int i = 0; i < 9; i++) u[i] = ubi[i];
+        lsq_update_exact(R, H, u);
+        for (int i = 0; i < 9; i++) ubi[i] = u[i];
+        *n_out = (int)nn;
+        *mean_out = nn > 0 ? ddiv(t[15], (double)nn) : 0.;
+    }
+}
+
+// ------------------------------------------------------- score_and_assign ----
+// ImageD11 src/closest.c:366-397, elementwise and bit-exact.
+__global__ void __launch_bounds__(kThreads)
+k_score_and_assign(const double* __restrict__ ubi, const double* __restrict__ gv,
+                   double tolsq, double* __restrict__ drlv2, int* __restrict__ labels,
+                   int label, int64_t ng, int* __restrict__ count) {
+    double u[9];
+    load_ubi(ubi, u);
+    int n = 0;
+    for (int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x; k < ng;
+         k += (int64_t)gridDim.x * kThreads) {
+        double ih[3];
+        double s = drlv2_exact(u, __ldg(gv + 3 * k), __ldg(gv + 3 * k + 1),
+                               __ldg(gv + 3 * k + 2), ih);
+        if ((s < tolsq) && (s < drlv2[k])) {
+            labels[k] = label;
+            drlv2[k] = s;
+            n++;
+        } else if (labels[k] == label) {
+            labels[k] = -1;
+        }
+    }
+    n = warp_sum(n);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(count, n);
+}
+
+// -------------------------------------------------------- verify_rounding ----
+// ImageD11 src/closest.c:100-119 with the device's rounding.
+__global__ void k_verify_rounding(int n, int* __restrict__ bad) {
+    int b = 0;
+    for (int i = threadIdx.x; i < 600; i += blockDim.x) {
+        int pass = i / 300, ii = i % 300 - 100;
+        double v = dadd((double)(pass == 0 ? n : -n), dmul((double)ii, 50.0));
+        int fast = (int)dround(v);
+        int slow = (int)floor(dadd(v, 0.5));
+        b += (fast != slow);
+    }
+    b = warp_sum(b);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(bad, b);
+}
+
+// ------------------------------------------ plain batched FP64 (baseline) ----
+// counts[m*ntol + j] += #{k : drlv2(ubis[m], g_k) < tolsq[j]}.  CTA b handles
+// UBI b / chunks and g range (b % chunks); one thread per g, grid-stride over
+// the range; warp sums + one atomic per warp.  The straightforward GPU port of
+// a loop of reference score() calls; all decisions bit-exact.
+struct TolSq {
+    double t[ID11B_MAX_TOLS];
+};
+
+__global__ void __launch_bounds__(kThreads)
+k_score_many_fp64(const double* __restrict__ ubis, int64_t m, const double* __restrict__ gv,
+                  int64_t ng, TolSq tolsq, int ntol, int chunks, int* __restrict__ counts) {
+    const int64_t ui = blockIdx.x / chunks;
+    const int c = blockIdx.x % chunks;
+    if (ui >= m) return;
+    const int64_t per = (ng + chunks - 1) / chunks;
+    const int64_t k0 = c * per, k1 = min(ng, k0 + per);
+    double u[9];
+    load_ubi(ubis + 9 * ui, u);
+    int cnt[ID11B_MAX_TOLS] = {0, 0, 0, 0};
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += kThreads) {
+        double ih[3];
+        double s = drlv2_exact(u, __ldg(gv + 3 * k), __ldg(gv + 3 * k + 1),
+                               __ldg(gv + 3 * k + 2), ih);
+#pragma unroll
+        for (int j = 0; j < ID11B_MAX_TOLS; j++)
+            if (j < ntol) cnt[j] += (s < tolsq.t[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < ID11B_MAX_TOLS; j++) {
+        if (j >= ntol) break;
+        int v = warp_sum(cnt[j]);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(counts + ui * ntol + j, v);
+    }
+}
+
+static int sm_count() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+static int stream_grid(int64_t ng, int per_sm) {
+    int64_t b = (ng + kThreads - 1) / kThreads;
+    int64_t cap = (int64_t)sm_count() * per_sm;
+    if (b > cap) b = cap;
+    return (int)(b > 0 ? b : 1);
+}
+
+// LSQ partial CTAs: a deterministic function of ng only (not of the device),
+// so a given input always reduces in the same order.
+static int lsq_blocks(int64_t ng) {
+    int64_t b = (ng + 4 * kThreads - 1) / (4 * kThreads);
+    if (b > kLsqMaxBlocks) b = kLsqMaxBlocks;
+    return (int)(b > 0 ? b : 1);
+}
+
+}  // namespace id11b
+
+using namespace id11b;
+
+extern "C" int64_t id11b_lsq_workspace_bytes(int64_t ng) {
+    (void)ng;
+    return (int64_t)kLsqMaxBlocks * (int64_t)sizeof(LsqPartial);
+}
+
+extern "C" int id11b_dev_score(const double* ubi, const double* gv, double tol, int64_t ng,
+                               int32_t* count, void* stream) {
+    if (ng < 0 || !ubi || !count || (ng > 0 && !gv)) return ID11B_ERR_ARG;
+    if (ng > INT32_MAX) return ID11B_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    ID11B_CHECK(cudaMemsetAsync(count, 0, sizeof(int32_t), st));
+    if (ng == 0) return ID11B_OK;
+    k_score<<<stream_grid(ng, 8), kThreads, 0, st>>>(ubi, gv, tol * tol, ng, count);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+static int lsq_launch(int mode, double* ubi, const double* gv, double tol,
+                      const int32_t* labels, int label, int64_t ng, int32_t* n,
+                      double* mean, void* ws, int64_t ws_bytes, void* stream) {
+    if (ng < 0 || !ubi || !n || !mean || !ws || (ng > 0 && !gv)) return ID11B_ERR_ARG;
+    if (mode == 1 && ng > 0 && !labels) return ID11B_ERR_ARG;
+    if (ng > INT32_MAX) return ID11B_ERR_SIZE;
+    if (ws_bytes < id11b_lsq_workspace_bytes(ng)) return ID11B_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    LsqPartial* part = (LsqPartial*)ws;
+    int nb = lsq_blocks(ng);
+    if (ng == 0) {
+        ID11B_CHECK(cudaMemsetAsync(part, 0, sizeof(LsqPartial), st));
+    } else if (mode == 0) {
+        k_lsq_partials<0><<<nb, kThreads, 0, st>>>(ubi, gv, tol * tol, nullptr, 0, ng, part);
+    } else {
+        k_lsq_partials<1><<<nb, kThreads, 0, st>>>(ubi, gv, 0., labels, label, ng, part);
+    }
+    ID11B_CHECK_LAUNCH();
+    k_lsq_finish<<<1, kThreads, 0, st>>>(part, ng == 0 ? 1 : nb, ubi, n, mean);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+extern "C" int id11b_dev_score_and_refine(double* ubi, const double* gv, double tol,
+                                          int64_t ng, int32_t* n, double* mean_drlv2,
+                                          void* workspace, int64_t workspace_bytes,
+                                          void* stream) {
+    return lsq_launch(0, ubi, gv, tol, nullptr, 0, ng, n, mean_drlv2, workspace,
+                      workspace_bytes, stream);
+}
+
+extern "C" int id11b_dev_refine_assigned(double* ubi, const double* gv,
+                                         const int32_t* labels, int label, int64_t ng,
+                                         int32_t* npk, double* mean_drlv2, void* workspace,
+                                         int64_t workspace_bytes, void* stream) {
+    return lsq_launch(1, ubi, gv, 0., labels, label, ng, npk, mean_drlv2, workspace,
+                      workspace_bytes, stream);
+}
+
+extern "C" int id11b_dev_score_and_assign(const double* ubi, const double* gv, double tol,
+                                          double* drlv2, int32_t* labels, int label,
+                                          int64_t ng, int32_t* count, void* stream) {
+    if (ng < 0 || !ubi || !count || (ng > 0 && (!gv || !drlv2 || !labels)))
+        return ID11B_ERR_ARG;
+    if (ng > INT32_MAX) return ID11B_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    ID11B_CHECK(cudaMemsetAsync(count, 0, sizeof(int32_t), st));
+    if (ng == 0) return ID11B_OK;
+    k_score_and_assign<<<stream_grid(ng, 8), kThreads, 0, st>>>(ubi, gv, tol * tol, drlv2,
+                                                                 labels, label, ng, count);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+extern "C" int id11b_dev_verify_rounding(int n, int32_t* bad, void* stream) {
+    if (!bad) return ID11B_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    ID11B_CHECK(cudaMemsetAsync(bad, 0, sizeof(int32_t), st));
+    k_verify_rounding<<<1, 320, 0, st>>>(n, bad);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+extern "C" int id11b_dev_score_many_fp64(const double* ubis, int64_t m, const double* gv,
+                                         int64_t ng, const double* tols_host, int ntol,
+                                         int32_t* counts, void* stream) {
+    if (m < 0 || ng < 0 || ntol < 1 || ntol > ID11B_MAX_TOLS || !tols_host || !counts)
+        return ID11B_ERR_ARG;
+    if ((m > 0 && !ubis) || (ng > 0 && !gv)) return ID11B_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    ID11B_CHECK(cudaMemsetAsync(counts, 0, sizeof(int32_t) * m * ntol, st));
+    if (m == 0 || ng == 0) return ID11B_OK;
+    TolSq ts;
+    for (int j = 0; j < ID11B_MAX_TOLS; j++) ts.t[j] = j < ntol ? tols_host[j] * tols_host[j] : 0.;
+    // g range per CTA: 64 g per thread, so CTA start-up stays a small part of
+    // each CTA's time, and M x chunks CTAs fill every SM many times over.
+    int64_t chunks = (ng + 64 * kThreads - 1) / (64 * kThreads);
+    if (chunks < 1) chunks = 1;
+    if (m * chunks > INT32_MAX) return ID11B_ERR_SIZE;
+    k_score_many_fp64<<<(unsigned)(m * chunks), kThreads, 0, st>>>(ubis, m, gv, ng, ts, ntol,
+                                                                  (int)chunks, counts);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}

@@ -1,0 +1,158 @@
+/*
+ * imaged11_b200 -- C ABI of the B200 (sm_100a) grain-scoring path.
+ *
+ * Two layers:
+ *
+ *  1. Reference-signature entry points (id11b_<name>): the exact C signatures
+ *     that ImageD11's f2py module binds (src/_cImageD11.pyf), with HOST
+ *     pointers.  Each call copies its inputs to the GPU, runs the kernels and
+ *     copies the results back before returning, so a binding that today points
+ *     at ImageD11's src/closest.c / src/cdiffraction.c can point here instead.
+ *     Device memory is taken from the CUDA stream-ordered pool on the calling
+ *     thread's per-thread default stream, so concurrent calls from different
+ *     host threads are safe (the reference marks score_and_refine and
+ *     refine_assigned "threadsafe").
+ *
+ *  2. Device entry points (id11b_dev_<name>): DEVICE pointers for every array,
+ *     scalars by value, small fixed-size parameter vectors (t[3], p[4], r[9],
+ *     dist[3]) as HOST pointers read during the call, and a cudaStream_t passed
+ *     as void*.  They only enqueue work; nothing is synchronised.  Kernels that
+ *     need scratch memory take a caller-provided workspace whose size is given
+ *     by the matching *_workspace_bytes() query.
+ *
+ * Every entry point returns an int status (ID11B_OK == 0) except where the
+ * reference's own signature returns a value; those report failure as noted.
+ * Scalar FP64 arithmetic that decides an assignment (rounding to hkl, the
+ * strict drlv2 < tol^2 test) is bit-exact with the reference C.
+ */
+#ifndef IMAGED11_B200_H
+#define IMAGED11_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define ID11B_OK 0
+#define ID11B_ERR_ARG 1     /* bad argument (negative size, null pointer, ntol > 4) */
+#define ID11B_ERR_CUDA 2    /* a CUDA call failed: see id11b_last_cuda_error()   */
+#define ID11B_ERR_ALIGN 3   /* pointer not aligned as the kernel requires        */
+#define ID11B_ERR_SIZE 4    /* size beyond a documented maximum                  */
+#define ID11B_ERR_TIMEOUT 5 /* a bounded device wait gave up                     */
+#define ID11B_ERR_NODEV 6   /* no CUDA device                                    */
+
+#define ID11B_MAX_TOLS 4
+
+/* ABI version (major*100 + minor). */
+int id11b_version(void);
+/* Human-readable text for a status code. */
+const char *id11b_status_string(int status);
+/* The cudaError_t behind the calling thread's last ID11B_ERR_CUDA. */
+int id11b_last_cuda_error(void);
+
+/* =====================================================================
+ * Layer 1: reference signatures, host pointers.
+ * ===================================================================== */
+
+/* Replaces compute_gv, ImageD11 src/cdiffraction.c:112-168
+ * (f2py: src/_cImageD11.pyf:551-564).  xlylzl (n,3), omega (n), t (3),
+ * gv (n,3) written.  Returns nothing, like the reference; failures are
+ * reported through id11b_last_status(). */
+void id11b_compute_gv(double xlylzl[][3], double omega[], double omegasign,
+                      double wvln, double wedge, double chi, double t[3],
+                      double gv[][3], int n);
+
+/* Replaces compute_geometry, ImageD11 src/cdiffraction.c:31-94
+ * (f2py: src/_cImageD11.pyf:534-549).  out (n,6) = tth, eta, ds, gx, gy, gz. */
+void id11b_compute_geometry(double xlylzl[][3], double omega[], double omegasign,
+                            double wvln, double wedge, double chi, double t[3],
+                            double out[][6], int n);
+
+/* Replaces compute_xlylzl, ImageD11 src/cdiffraction.c:190-224
+ * (f2py: src/_cImageD11.pyf:566-583).  p = [s_cen, f_cen, s_size, f_size],
+ * r (9) = detector rotation . flip, row-major; dist (3). */
+void id11b_compute_xlylzl(double s[], double f[], double p[4], double r[9],
+                          double dist[3], double xlylzl[][3], int n);
+
+/* Replaces score, ImageD11 src/closest.c:227-248 (f2py: src/_cImageD11.pyf:106-120).
+ * Returns the count, or -1 on failure (see id11b_last_status()). */
+int id11b_score(double ubi[3][3], double gv[][3], double tol, int ng);
+
+/* Replaces score_and_refine, ImageD11 src/closest.c:267-345
+ * (f2py: src/_cImageD11.pyf:123-136).  ubi is refined in place; *n_arg and
+ * *sumdrlv2_arg receive the count and mean drlv2 before the update. */
+void id11b_score_and_refine(double ubi[3][3], double gv[][3], double tol,
+                            int *n_arg, double *sumdrlv2_arg, int ng);
+
+/* Replaces refine_assigned, ImageD11 src/closest.c:416-474
+ * (f2py: src/_cImageD11.pyf:156-170).  Uses peaks with labels[k] == label. */
+void id11b_refine_assigned(double ubi[3][3], double gv[][3], int labels[], int label,
+                           int *npk, double *sumdrlv2, int ng);
+
+/* Replaces score_and_assign, ImageD11 src/closest.c:366-397
+ * (f2py: src/_cImageD11.pyf:138-154).  drlv2 and labels updated in place.
+ * Returns the count, or -1 on failure. */
+int id11b_score_and_assign(double ubi[3][3], double gv[][3], double tol,
+                           double drlv2[], int labels[], int label, int ng);
+
+/* Replaces verify_rounding, ImageD11 src/closest.c:100-119
+ * (f2py: src/_cImageD11.pyf:69-74): runs the check
+ * with the GPU's rounding.  Returns the number of mismatches (0 = good), or
+ * -1 on failure. */
+int id11b_verify_rounding(int n);
+
+/* Status of the calling thread's last layer-1 call. */
+int id11b_last_status(void);
+
+/* =====================================================================
+ * Layer 2: device pointers + stream.
+ * ===================================================================== */
+
+/* compute_gv on device arrays.  If g4 is non-null it also receives an FP32
+ * copy of every g as (gx, gy, gz, 0) float4 for the batched scorers (16-byte
+ * aligned). */
+int id11b_dev_compute_gv(const double *xlylzl, const double *omega, double omegasign,
+                         double wvln, double wedge, double chi, const double *t_host,
+                         double *gv, float *g4, int64_t n, void *stream);
+
+int id11b_dev_compute_geometry(const double *xlylzl, const double *omega,
+                               double omegasign, double wvln, double wedge, double chi,
+                               const double *t_host, double *out, int64_t n,
+                               void *stream);
+
+int id11b_dev_compute_xlylzl(const double *s, const double *f, const double *p_host,
+                             const double *r_host, const double *dist_host,
+                             double *xlylzl, int64_t n, void *stream);
+
+/* score: *count (device int32) = number of g with drlv2 < tol^2. */
+int id11b_dev_score(const double *ubi, const double *gv, double tol, int64_t ng,
+                    int32_t *count, void *stream);
+
+/* Workspace for dev_score_and_refine / dev_refine_assigned. */
+int64_t id11b_lsq_workspace_bytes(int64_t ng);
+
+/* score_and_refine on device: ubi (9, device) refined in place; *n (int32)
+ * and *mean_drlv2 (double) written on the device. */
+int id11b_dev_score_and_refine(double *ubi, const double *gv, double tol, int64_t ng,
+                               int32_t *n, double *mean_drlv2, void *workspace,
+                               int64_t workspace_bytes, void *stream);
+
+int id11b_dev_refine_assigned(double *ubi, const double *gv, const int32_t *labels,
+                              int label, int64_t ng, int32_t *npk, double *mean_drlv2,
+                              void *workspace, int64_t workspace_bytes, void *stream);
+
+/* score_and_assign on device; *count (int32, device) receives the count. */
+int id11b_dev_score_and_assign(const double *ubi, const double *gv, double tol,
+                               double *drlv2, int32_t *labels, int label, int64_t ng,
+                               int32_t *count, void *stream);
+
+/* verify_rounding on the device; *bad (int32, device) = mismatches. */
+int id11b_dev_verify_rounding(int n, int32_t *bad, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMAGED11_B200_H */

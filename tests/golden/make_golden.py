@@ -1,0 +1,244 @@
+"""Generate the golden fixtures in tests/golden/ from the REFERENCE itself.
+
+Run in a container that has the reference checkout (default /root/reference):
+
+    make -C oracle            # builds oracle/_ref/libimaged11_ref.so from the
+                              # reference's own src/closest.c, src/cdiffraction.c
+    python tests/golden/make_golden.py [/path/to/reference]
+
+Outputs come from two reference implementations:
+
+* the reference's compiled C (unmodified sources, via oracle/_ref) for every
+  hot-path function: compute_gv, compute_geometry, compute_xlylzl, score,
+  score_and_refine, refine_assigned, score_and_assign;
+* the reference's numpy module ImageD11/transform.py (compute_tth_eta_from_xyz
+  + compute_g_vectors, compute_xyz_lab, detector_rotation_matrix), imported
+  with stub ``fabio``/``cImageD11`` modules because only its numpy functions
+  are used.
+
+Inputs: the cases of the reference's own test/test_cImageD11.py (7 wedge /
+chi / translation / omegasign sets on 203 points; 8 detector flips x 27 tilt
+triples), seeded synthetic peak sets from imaged11_b200.synth, and adversarial
+scoring cases (fractional parts at 0.5 +- k ulp, drlv2 at tol^2 +- ulp,
+singular normal matrices, non-finite and huge g-vectors).
+
+The fixtures are small .npz files committed beside this script; the tests
+read only the .npz files, never the reference.
+"""
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, REPO)
+
+from oracle.oracle import Reference  # noqa: E402
+from imaged11_b200 import synth  # noqa: E402
+
+
+def import_reference_transform(ref_root):
+    """ImageD11.transform with stubbed heavy imports (fabio, cImageD11)."""
+    sys.modules.setdefault("fabio", types.ModuleType("fabio"))
+    pkg = types.ModuleType("ImageD11")
+    pkg.__path__ = [os.path.join(ref_root, "ImageD11")]
+    sys.modules["ImageD11"] = pkg
+    cim = types.ModuleType("ImageD11.cImageD11")
+    sys.modules["ImageD11.cImageD11"] = cim
+    pkg.cImageD11 = cim
+    import importlib
+    gvg = importlib.import_module("ImageD11.gv_general")
+    pkg.gv_general = gvg
+    return importlib.import_module("ImageD11.transform")
+
+
+def cases_compute_gv(ref, tr):
+    """test/test_cImageD11.py:14-128 inputs, plus a seeded random set."""
+    N = 203
+    XLYLZL = np.array([np.linspace(0, 2000, N), np.linspace(10, 2010, N), np.ones(N)])
+    omega = np.linspace(-180, 180, N)
+    params = [  # wedge, chi, omegasign, wvln, t_x, t_y, t_z
+        (5., 10., 1.0, 0.125, 20., 30., 40.),
+        (5., 0., 1.0, 0.125, 20., 30., 40.),
+        (0., 5., 1.0, 0.125, 20., 30., 40.),
+        (5., 10., -1.0, 0.125, 200., 300., 40.),
+        (5., 0., 1.0, 0.125, 200., 300., -400.),
+        (0., 0., 1.0, 0.125, 0., 0., 0.),
+        (0., 0., 1.0, 0.125, 200., 300., 400.),
+    ]
+    out = {}
+    for i, (w, c, osg, wl, tx, ty, tz) in enumerate(params):
+        t = np.array([tx, ty, tz])
+        gv = ref.compute_gv(XLYLZL.T.copy(), omega, osg, wl, w, c, t)
+        tth, eta = tr.compute_tth_eta_from_xyz(XLYLZL, omega * osg, t_x=tx, t_y=ty, t_z=tz,
+                                               wedge=w, chi=c)
+        gnp = tr.compute_g_vectors(tth, eta, omega * osg, wl, wedge=w, chi=c).T
+        geom = ref.compute_geometry(XLYLZL.T.copy(), omega, osg, wl, w, c, t)
+        out["gv%d_params" % i] = np.array([osg, wl, w, c, tx, ty, tz])
+        out["gv%d_out" % i] = gv
+        out["gv%d_numpy" % i] = gnp
+        out["gv%d_geometry" % i] = geom
+    out["gv_xlylzl"] = XLYLZL.T.copy()
+    out["gv_omega"] = omega
+    out["gv_ncases"] = np.array(len(params))
+    # seeded random lab positions on a realistic detector, nonzero wedge/chi/t
+    rng = np.random.default_rng(20240611)
+    n = 4096
+    x = np.stack([rng.uniform(1.4e5, 1.6e5, n), rng.uniform(-8e4, 8e4, n),
+                  rng.uniform(-8e4, 8e4, n)], 1)
+    om = rng.uniform(-180, 360, n)
+    t = np.array([5., -3., 2.])
+    out["rand_xlylzl"] = x
+    out["rand_omega"] = om
+    out["rand_params"] = np.array([-1.0, 0.2846, 0.01, 0.02, 5., -3., 2.])
+    out["rand_gv"] = ref.compute_gv(x, om, -1.0, 0.2846, 0.01, 0.02, t)
+    out["rand_geometry"] = ref.compute_geometry(x, om, -1.0, 0.2846, 0.01, 0.02, t)
+    return out
+
+
+def cases_xlylzl(ref, tr):
+    """test/test_cImageD11.py:132-190: 8 flips x 27 tilts."""
+    rng = np.random.default_rng(7)
+    npk = 64
+    sc = rng.random(npk) * 2048
+    fc = rng.random(npk) * 2048
+    pars = dict(z_center=980., y_center=1010., z_size=48., y_size=49., distance=100100.)
+    p = np.array([pars["z_center"], pars["y_center"], pars["z_size"], pars["y_size"]])
+    dist = np.array([pars["distance"], 0., 0.])
+    tilts = [(x, y, z) for x in (-0.5, 0., 0.24) for y in (-0.5, 0., 0.24)
+             for z in (-0.5, 0., 0.24)]
+    flips = [[1, 0, 0, 1], [-1, 0, 0, 1], [-1, 0, 0, -1], [1, 0, 0, -1],
+             [0, 1, 1, 0], [0, -1, 1, 0], [0, -1, -1, 0], [0, 1, -1, 0]]
+    R, OUT, NP = [], [], []
+    for o11, o12, o21, o22 in flips:
+        for tx, ty, tz in tilts:
+            kw = dict(pars, tilt_x=tx, tilt_y=ty, tilt_z=tz, o11=o11, o12=o12, o21=o21, o22=o22)
+            dmat = tr.detector_rotation_matrix(tx, ty, tz)
+            fmat = np.array([[1, 0, 0], [0, o22, o21], [0, o12, o11]], float)
+            r = np.dot(dmat, fmat)
+            R.append(r.ravel())
+            OUT.append(ref.compute_xlylzl(sc, fc, p, r.ravel(), dist))
+            NP.append(tr.compute_xyz_lab((sc, fc), **kw).T)
+    return dict(xl_s=sc, xl_f=fc, xl_p=p, xl_dist=dist, xl_r=np.array(R), xl_out=np.array(OUT),
+                xl_numpy=np.array(NP))
+
+
+def adversarial_gv(ubi, rng):
+    """g-vectors that put h = UBI.g exactly on rounding / tolerance edges."""
+    ub = np.linalg.inv(ubi)
+    hs = []
+    base = rng.integers(-6, 7, size=(64, 3)).astype(float)
+    # fractional parts at +-0.5 and a few ulps either side
+    for k in (-3, -1, 0, 1, 3):
+        h = base.copy()
+        h[:, 0] = np.floor(h[:, 0]) + 0.5
+        h[:, 0] = h[:, 0] + k * np.spacing(h[:, 0])
+        hs.append(h)
+    # drlv2 == tol^2 (+- ulp) on one component for tol in (0.02, 0.05, 0.1)
+    for tol in (0.02, 0.05, 0.1):
+        for k in (-2, -1, 0, 1, 2):
+            h = base.copy()
+            h[:, 1] = h[:, 1] + tol + k * np.spacing(tol)
+            hs.append(h)
+    h = np.concatenate(hs)
+    g = h @ ub.T
+    # back-solve so that UBI.g lands as close as possible in FP64
+    return g
+
+
+def cases_scoring(ref):
+    out = {}
+    # realistic scene: FCC Al, 40 grains, noise peaks, cfg0-like geometry
+    ps = synth.simulate(40, "Al", gmax=1.2, seed=11, noise_frac=0.10)
+    gv = ps.gv
+    rng = np.random.default_rng(12)
+    ubis = np.concatenate([synth.perturb_ubis(ps.ubis[:20], 0.1, 0.001, rng),
+                           synth.trial_ubis(ps.ubis, 12, 0.0, 0.0, rng),
+                           ps.ubis[20:24]])
+    tols = np.array([0.02, 0.05, 0.1, 0.25])
+    out["sc_gv"] = gv
+    out["sc_ubis"] = ubis
+    out["sc_tols"] = tols
+    out["sc_counts"] = np.array([[ref.score(u, gv, t) for t in tols] for u in ubis], np.int32)
+    n, d, u2 = [], [], []
+    for u in ubis:
+        for t in tols:
+            a, b, c = ref.score_and_refine(u, gv, t)
+            n.append(a); d.append(b); u2.append(c)
+    out["sar_n"] = np.array(n, np.int32).reshape(len(ubis), len(tols))
+    out["sar_drlv2"] = np.array(d).reshape(len(ubis), len(tols))
+    out["sar_ubi"] = np.array(u2).reshape(len(ubis), len(tols), 3, 3)
+    # three iterations of score_and_refine per UBI at tol 0.05 (cfg0 procedure)
+    it = []
+    for u in ubis[:20]:
+        uu = u.copy()
+        for _ in range(3):
+            _, _, uu = ref.score_and_refine(uu, gv, 0.05)
+        it.append(uu)
+    out["sar3_ubi"] = np.array(it)
+    # refine_assigned over the true labels
+    labels = ps.labels.astype(np.int32)
+    ra_n, ra_d, ra_u = [], [], []
+    for gi in range(8):
+        a, b, c = ref.refine_assigned(ubis[gi], gv, labels, gi)
+        ra_n.append(a); ra_d.append(b); ra_u.append(c)
+    out["ra_labels"] = labels
+    out["ra_n"] = np.array(ra_n, np.int32)
+    out["ra_drlv2"] = np.array(ra_d)
+    out["ra_ubi"] = np.array(ra_u)
+    # score_and_assign, sequentially over the first 24 UBIs (as refinegrains.assignlabels)
+    drl = np.full(len(gv), 2.0)
+    lab = np.full(len(gv), -1, np.int32)
+    sa_n = []
+    for i, u in enumerate(ubis[:24]):
+        k, drl, lab = ref.score_and_assign(u, gv, 0.05, drl, lab, i)
+        sa_n.append(k)
+    out["sa_n"] = np.array(sa_n, np.int32)
+    out["sa_drlv2"] = drl
+    out["sa_labels"] = lab
+    # adversarial boundary set
+    u0 = ps.ubis[0]
+    g_adv = adversarial_gv(u0, rng)
+    specials = np.array([[np.nan, 0.1, 0.2], [np.inf, 0., 0.], [0., -np.inf, 1.],
+                         [1e30, 1e30, -1e30], [3e15, 1., 2.], [0., 0., 0.]])
+    g_adv = np.concatenate([g_adv, specials])
+    out["adv_gv"] = g_adv
+    out["adv_ubi"] = u0
+    out["adv_counts"] = np.array([ref.score(u0, g_adv, t) for t in tols], np.int32)
+    an, ad, au = [], [], []
+    for t in tols:
+        a, b, c = ref.score_and_refine(u0, g_adv[:-6], t)
+        an.append(a); ad.append(b); au.append(c)
+    out["adv_sar_n"] = np.array(an, np.int32)
+    out["adv_sar_drlv2"] = np.array(ad)
+    out["adv_sar_ubi"] = np.array(au)
+    # singular / degenerate refinement: 0, 1, 2 peaks and coplanar peaks
+    sing = []
+    h_sets = [np.zeros((0, 3)), np.array([[1., 1, 1]]), np.array([[1., 1, 1], [2, 0, 0]]),
+              np.array([[1., 1, 1], [2, 0, 0], [1, -1, -1], [3, 1, 1]])]
+    for i, hset in enumerate(h_sets):
+        g = hset @ np.linalg.inv(u0).T
+        a, b, c = ref.score_and_refine(u0, g, 0.05)
+        sing.append(np.concatenate([[a, b], c.ravel()]))
+        out["sing%d_gv" % i] = g.reshape(-1, 3)
+    out["sing_results"] = np.array(sing)
+    return out
+
+
+def main():
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = Reference()
+    tr = import_reference_transform(ref_root)
+    assert ref.verify_rounding(20) == 0
+    np.savez_compressed(os.path.join(HERE, "compute_gv.npz"), **cases_compute_gv(ref, tr))
+    np.savez_compressed(os.path.join(HERE, "compute_xlylzl.npz"), **cases_xlylzl(ref, tr))
+    np.savez_compressed(os.path.join(HERE, "scoring.npz"), **cases_scoring(ref))
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,378 @@
+"""Benchmark: batched candidate-grain scoring on B200.
+
+Workload (default): 1.1M g-vectors simulated from 2,000 FCC Al grains
+(a = 4.05 A, |g| <= 1.5 A^-1, wavelength 0.2846 A, 150 mm, 2048^2 x 75 um
+detector, sigma 0.5 px / 0.05 deg centroid noise, 10% uniform noise peaks)
+scored against 20,000 trial UBIs (10% true orientations perturbed by 0.5 deg,
+90% uniformly random orientations of the same cell) at tol = 0.02, 0.05, 0.1
+in one launch sequence, counts identical to the reference's score().
+
+Metric: assigned peak x grain pairs per second = M * N * T / step time.
+One step = FP32 copy of the g-vectors + batched score (UBI packing, screening
+kernel, exact-FP64 list kernel), inputs resident in HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun): every rank scores its own 20,000 trial UBIs against the
+same g-vectors (weak scaling, no collective on the data path); the step time
+is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+TOLS = [0.02, 0.05, 0.1]
+N_GRAINS = 2000
+GMAX = 1.5
+N_UBI = 20000
+SEED = 1234
+FLOP_PER_EVAL = 30   # per (UBI, g): 9 FMA (18), 3 rint, 3 sub, 5 for t.t, 1 compare
+L2_FLUSH_BYTES = 256 << 20
+
+
+def measured_hbm_peak():
+    """Measured HBM copy bandwidth for this GPU pool (GB/s), else the fallback."""
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def compute_gv_measure(torch, ps, dev, n_peaks=10_000_000, steps=5, flush=None):
+    """compute_gv (FP64 drop-in kernel) over n_peaks lab positions, inputs
+    resident; returns (GB/s of algorithmic traffic, ms per launch)."""
+    from imaged11_b200 import cImageD11 as cim
+    reps = (n_peaks + len(ps.xyz) - 1) // len(ps.xyz)
+    x = torch.tensor(ps.xyz, device=dev).repeat(reps, 1)[:n_peaks].contiguous()
+    om = torch.tensor(ps.omega, device=dev).repeat(reps)[:n_peaks].contiguous()
+    g = torch.empty_like(x)
+    geo = ps.geo
+
+    def run():
+        cim.compute_gv(x, om, geo["omegasign"], geo["wavelength"], geo["wedge"], geo["chi"],
+                       [0.0, 0.0, 0.0], g)
+    for _ in range(3):
+        run()
+    times = cuda_time_ms(torch, run, steps, flush)
+    ms = float(np.mean(times))
+    return 56.0 * n_peaks / (ms * 1e-3) / 1e9, ms
+
+
+def workload(rank=0, n_ubi=N_UBI):
+    from imaged11_b200 import synth
+    ps = synth.simulate(N_GRAINS, "Al", gmax=GMAX, seed=SEED, noise_frac=0.10)
+    rng = np.random.default_rng(SEED + 1 + rank)
+    ubis = synth.trial_ubis(ps.ubis, n_ubi, 0.10, 0.5, rng)
+    return ps, ubis
+
+
+def config_dict(n, m):
+    return {
+        "workload": "batched candidate scoring: %d g-vectors (2000 FCC Al grains, |g|<=%.1f, "
+                    "10%% noise peaks) x %d trial UBIs x tols %s" % (n, GMAX, m, TOLS),
+        "n_gvectors": n, "n_ubis_per_gpu": m, "tols": TOLS, "seed": SEED,
+        "pairs_per_step": "M*N*T", "l2": "flushed between timed steps (256 MB write)",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cuda_time_ms(torch, fn, steps, flush=None):
+    """Per-step CUDA-event times (ms) on the current stream, L2 flushed between."""
+    times = []
+    st = torch.cuda.current_stream()
+    for _ in range(steps):
+        if flush is not None:
+            flush()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
+def cpu_reference_rate(ps, ubis, seconds=10.0, kind="reference"):
+    """The reference's own C score() over UBIs (OpenMP, all host threads) on a
+    bounded sample of the workload; pairs/s."""
+    from oracle import oracle as orc
+    lib = orc.Reference() if (kind == "reference" and orc.have_reference()) else orc.Oracle()
+    kind = "reference" if isinstance(lib, orc.Reference) else "port"
+    gv = np.ascontiguousarray(ps.gv)
+    cores = lib.max_threads()
+    # calibrate on a few UBIs, then size the sample to about `seconds`
+    k = max(cores, 8)
+    t0 = time.perf_counter()
+    lib.score_many(ubis[:k], gv, TOLS)
+    dt = time.perf_counter() - t0
+    m = int(min(len(ubis), max(k, k * seconds / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    lib.score_many(ubis[:m], gv, TOLS)
+    dt = time.perf_counter() - t0
+    pairs = m * len(gv) * len(TOLS)
+    return {"value": pairs / dt, "unit": "pairs/s", "cores": cores, "kind": kind,
+            "sample": "%d UBIs x %d g x %d tols (%.1f s)" % (m, len(gv), len(TOLS), dt)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    ps, ubis = workload()
+    from oracle import oracle as orc
+    lib = orc.Reference() if orc.have_reference() else orc.Oracle()
+    kind = "reference" if isinstance(lib, orc.Reference) else "port"
+    gv = np.ascontiguousarray(ps.gv)
+    cores = lib.max_threads()
+    m = max(cores * 4, 64)         # each step: a bounded sample of the workload
+    for _ in range(args.warmup):
+        lib.score_many(ubis[:m], gv, TOLS)
+    times = []
+    for i in range(args.steps):
+        u = ubis[(i * m) % (len(ubis) - m):][:m]
+        t0 = time.perf_counter()
+        lib.score_many(u, gv, TOLS)
+        times.append(time.perf_counter() - t0)
+    pairs = m * len(gv) * len(TOLS)
+    value = pairs * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": "assigned peak x grain pairs/s", "value": value,
+        "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(len(gv), N_UBI),
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": kind,
+                         "sample": "%d UBIs x %d g x %d tols per step" % (m, len(gv), len(TOLS))},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from imaged11_b200 import batch
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ps, ubis = workload(rank, args.ubis)
+    if args.case == "gv":       # compute_gv alone (profiling case)
+        gbs, ms = compute_gv_measure(torch, ps, dev, args.peaks, args.steps)
+        print(json.dumps({"case": "compute_gv", "peaks": args.peaks, "GB/s": gbs, "ms": ms}))
+        return 0
+    n, m, T = len(ps.gv), len(ubis), len(TOLS)
+    pairs = m * n * T
+
+    gv_d = torch.tensor(ps.gv, device=dev)
+    ubis_d = torch.tensor(ubis, device=dev)
+    gs = batch.GvecSet(gv_d)
+    ws = batch.BatchWorkspace(m, n, refine=False)
+    counts = torch.empty((m, T), dtype=torch.int32, device=dev)
+    flush_buf = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def flush():
+        flush_buf.fill_(1)
+
+    def step():
+        gs.prepare()
+        batch.score_batch(ubis_d, gs, TOLS, workspace=ws, out=counts)
+
+    # correctness spot-check against the plain FP64 kernel (same assignments)
+    step()
+    c64 = batch.score_many_fp64(ubis_d[:512], gs, TOLS)
+    assert torch.equal(c64, counts[:512]), "FP32+recheck counts differ from FP64"
+    if args.kernel_only:        # profiling case: warm-up + timed steps, nothing else
+        for _ in range(args.warmup + args.steps):
+            step()
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "score_batch", "ubis": m, "gvectors": n}))
+        return 0
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        times = cuda_time_ms(torch, step, args.steps, flush)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t = torch.tensor([sum(times)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = pairs * world / (ms_per_step * 1e-3)
+
+    # the screening kernel alone (score_batch on prepared g-vectors)
+    k_times = cuda_time_ms(torch, lambda: batch.score_batch(ubis_d, gs, TOLS, workspace=ws,
+                                                           out=counts), max(2, args.steps), flush)
+    k_ms = float(np.mean(k_times))
+    nrecheck, nfallback = ws.stats()
+
+    # plain FP64 baseline: reference arithmetic, one launch per tolerance as
+    # the reference API scores one tolerance per call, and all tols at once
+    m64 = min(m, 2000)
+    p64_per_tol = cuda_time_ms(torch, lambda: [batch.score_many_fp64(ubis_d[:m64], gs, [t])
+                                               for t in TOLS], 2, flush)
+    p64_fused = cuda_time_ms(torch, lambda: batch.score_many_fp64(ubis_d[:m64], gs, TOLS), 2,
+                             flush)
+    rate64 = m64 * n * T / (np.mean(p64_per_tol) * 1e-3)
+    rate64f = m64 * n * T / (np.mean(p64_fused) * 1e-3)
+
+    # compute_gv (HBM-bound FP64 streaming kernel), 10M peaks
+    gv_gbs, gv_ms = compute_gv_measure(torch, ps, dev, 10_000_000, max(3, args.steps), flush)
+    hbm_peak, hbm_kind = measured_hbm_peak()
+
+    # end to end through the public API: pinned host inputs -> counts on host
+    gv_h = torch.tensor(ps.gv).pin_memory()
+    ub_h = torch.tensor(ubis).pin_memory()
+
+    def e2e_step():
+        g = batch.GvecSet(gv_h.to(dev, non_blocking=True))
+        c = batch.score_batch(ub_h.to(dev, non_blocking=True), g, TOLS, workspace=ws)
+        return c.cpu()
+
+    for _ in range(2):
+        e2e_step()
+    e2e_times = cuda_time_ms(torch, e2e_step, max(2, args.steps), flush)
+    e2e_ms = float(np.mean(e2e_times))
+    e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = pairs * world / (float(e2e_t.item()) * 1e-3)
+
+    if rank != 0:
+        return 0
+
+    clocks = clk.summary()
+    sm_mhz = clocks["sm_mhz"] or 1965.0
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp32_peak = nsm * 128 * 2 * sm_mhz * 1e6 / 1e12
+    achieved = (m * n * FLOP_PER_EVAL) / (k_ms * 1e-3) / 1e12
+    cpu = cpu_reference_rate(ps, ubis) if world == 1 else None
+    line = {
+        "metric": "assigned peak x grain pairs/s", "value": value, "unit": "pairs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64recheck", "data": "synthetic",
+        "config": config_dict(n, m),
+        "e2e": {"value": e2e_value, "unit": "pairs/s",
+                "h2d_bytes_per_step": int(ps.gv.nbytes + ubis.nbytes),
+                "d2h_bytes_per_step": int(m * T * 4)},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "kernel": "k_batch<4,3,score>",
+                     "peak_note": "CUDA-core FP32 = SMs x 128 x 2 x median SM clock under load; "
+                                  "%d FLOP per (UBI,g) evaluation" % FLOP_PER_EVAL},
+        "plain_fp64": {"value_per_tol_launch": rate64, "value_all_tols": rate64f,
+                       "unit": "pairs/s", "ubis": m64,
+                       "ratio_vs_per_tol": value / rate64, "ratio_vs_all_tols": value / rate64f},
+        "compute_gv": {"peaks": 10_000_000, "ms": gv_ms, "achieved_gbs": gv_gbs,
+                       "peak_gbs": hbm_peak, "peak_kind": hbm_kind,
+                       "frac": gv_gbs / hbm_peak, "bytes_per_peak": 56},
+        "recheck": {"fp64_pairs": nrecheck, "fraction": nrecheck / (m * n),
+                    "fallback_ubis": nfallback},
+        "gpu_launches": 4 * args.steps,
+        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ubis", type=int, default=N_UBI, help="trial UBIs per GPU")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="only warm-up + timed steps of the scoring step (profiling case)")
+    ap.add_argument("--case", default="score", choices=["score", "gv"],
+                    help="gv: compute_gv alone on --peaks lab positions (profiling case)")
+    ap.add_argument("--peaks", type=int, default=10_000_000)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

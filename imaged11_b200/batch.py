@@ -1,0 +1,161 @@
+"""Batched grain scoring and refinement on the GPU (beyond the per-call drop-in).
+
+The reference scores trial orientations one ``score`` call at a time
+(ImageD11/indexing.py:762-874, ``indexer.scorethem``) and refines grains one
+``score_and_refine`` call at a time (ImageD11/refinegrains.py:459-498).  These
+functions run whole batches in one launch sequence with identical
+assignments:
+
+* :class:`GvecSet` keeps a g-vector table resident on the GPU in FP64 plus the
+  FP32 float4 copy and screening metadata the batched kernels read;
+* :func:`score_batch` -- counts (and drlv2 sums) for M UBIs x T tolerances,
+  FP32 screening with exact FP64 recheck inside a proven error band;
+* :func:`score_many_fp64` -- the same counts from the plain FP64 kernel
+  (reference arithmetic, one thread per g), the baseline;
+* :func:`refine_batch` -- ``iters`` score_and_refine rounds for M UBIs against
+  all g-vectors.
+
+All tensors live on the current CUDA device; work is enqueued on the current
+stream.
+"""
+import numpy as np
+
+from ._lib import lib, check
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream():
+    return _torch().cuda.current_stream().cuda_stream
+
+
+def _dev(a, dtype):
+    torch = _torch()
+    if isinstance(a, torch.Tensor):
+        if not a.is_cuda:
+            a = a.cuda()
+        return a.to(dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda").to(dtype).contiguous()
+
+
+def _tols(tols):
+    t = np.ascontiguousarray(np.atleast_1d(tols), dtype=np.float64)
+    if t.ndim != 1 or not 1 <= len(t) <= 4:
+        raise ValueError("between 1 and 4 tolerances are supported per launch")
+    return t
+
+
+class GvecSet:
+    """g-vectors (n,3) float64 resident on the GPU with their FP32 copy.
+
+    ``gv`` may be a numpy array or a CUDA tensor; it is copied once."""
+
+    def __init__(self, gv):
+        torch = _torch()
+        self.gv = _dev(gv, torch.float64).reshape(-1, 3)
+        self.n = self.gv.shape[0]
+        self.g4 = torch.empty((max(self.n, 1), 4), dtype=torch.float32, device=self.gv.device)
+        wsb = lib.id11b_gvec_workspace_bytes(self.n)
+        self.ws = torch.empty(wsb, dtype=torch.uint8, device=self.gv.device)
+        self.prepare()
+
+    def prepare(self):
+        """(Re)build the FP32 copy and screening data from self.gv."""
+        check(lib.id11b_dev_prepare_gvecs(self.gv.data_ptr(), self.n, self.g4.data_ptr(),
+                                          self.ws.data_ptr(), self.ws.numel(), _stream()),
+              "prepare_gvecs")
+
+
+class BatchWorkspace:
+    """Reusable scratch for score_batch / refine_batch of a given size."""
+
+    def __init__(self, m, n, refine=False):
+        torch = _torch()
+        self.m, self.n, self.refine = m, n, int(bool(refine))
+        wsb = lib.id11b_batch_workspace_bytes(m, n, self.refine)
+        self.buf = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+
+    def fits(self, m, n, refine):
+        return lib.id11b_batch_workspace_bytes(m, n, int(bool(refine))) <= self.buf.numel()
+
+    def stats(self):
+        """(FP64 re-evaluations, UBIs evaluated wholly in FP64); raises on a
+        device error flag.  Synchronises the stream."""
+        import ctypes
+        nr = ctypes.c_int64(0)
+        nf = ctypes.c_int32(0)
+        er = ctypes.c_int32(0)
+        rc = lib.id11b_batch_stats(self.buf.data_ptr(), self.m, self.n, self.refine,
+                                   ctypes.addressof(nr), ctypes.addressof(nf),
+                                   ctypes.addressof(er), _stream())
+        check(rc, "batch")
+        return nr.value, nf.value
+
+
+def score_batch(ubis, gvs, tols, sums=False, workspace=None, out=None):
+    """Counts of g-vectors indexed by each UBI at each tolerance.
+
+    ubis: (m,3,3) float64 (numpy or CUDA); gvs: GvecSet; tols: 1-4 values.
+    Returns an int32 CUDA tensor (m, len(tols)) -- and, with sums=True, the
+    float64 tensor of summed drlv2 of the counted pairs."""
+    torch = _torch()
+    u = _dev(ubis, torch.float64).reshape(-1, 9)
+    m = u.shape[0]
+    t = _tols(tols)
+    ws = workspace if workspace is not None and workspace.fits(m, gvs.n, False) else \
+        BatchWorkspace(m, gvs.n, False)
+    counts = out if out is not None else torch.empty((m, len(t)), dtype=torch.int32,
+                                                     device=u.device)
+    s = torch.empty((m, len(t)), dtype=torch.float64, device=u.device) if sums else None
+    check(lib.id11b_dev_score_batch(u.data_ptr(), m, gvs.gv.data_ptr(), gvs.g4.data_ptr(),
+                                    gvs.n, gvs.ws.data_ptr(), t.ctypes.data, len(t),
+                                    counts.data_ptr(), s.data_ptr() if sums else None,
+                                    ws.buf.data_ptr(), ws.buf.numel(), _stream()),
+          "score_batch")
+    score_batch.last_workspace = ws
+    return (counts, s) if sums else counts
+
+
+def score_many_fp64(ubis, gv, tols, out=None):
+    """Plain FP64 batched score (reference arithmetic).  gv: (n,3) float64 CUDA
+    tensor or GvecSet.  Returns int32 (m, len(tols))."""
+    torch = _torch()
+    g = gv.gv if isinstance(gv, GvecSet) else _dev(gv, torch.float64).reshape(-1, 3)
+    u = _dev(ubis, torch.float64).reshape(-1, 9)
+    t = _tols(tols)
+    counts = out if out is not None else torch.empty((u.shape[0], len(t)), dtype=torch.int32,
+                                                     device=u.device)
+    check(lib.id11b_dev_score_many_fp64(u.data_ptr(), u.shape[0], g.data_ptr(), g.shape[0],
+                                        t.ctypes.data, len(t), counts.data_ptr(), _stream()),
+          "score_many_fp64")
+    return counts
+
+
+def refine_batch(ubis, gvs, tol, iters=1, workspace=None):
+    """``iters`` rounds of score_and_refine for every UBI against every g.
+
+    ubis: (m,3,3) float64 CUDA tensor, refined in place (a numpy array is
+    copied to the GPU and the refined copy returned).  Returns
+    (ubis, npk, mean_drlv2) of the last round."""
+    torch = _torch()
+    if isinstance(ubis, torch.Tensor) and ubis.is_cuda:
+        if ubis.dtype != torch.float64 or not ubis.is_contiguous():
+            raise ValueError("ubis: contiguous float64 CUDA tensor required")
+        u = ubis
+    else:
+        u = _dev(ubis, torch.float64)
+    u9 = u.view(-1, 9)
+    m = u9.shape[0]
+    ws = workspace if workspace is not None and workspace.fits(m, gvs.n, True) else \
+        BatchWorkspace(m, gvs.n, True)
+    npk = torch.zeros(m, dtype=torch.int32, device=u.device)
+    mean = torch.zeros(m, dtype=torch.float64, device=u.device)
+    check(lib.id11b_dev_refine_batch(u9.data_ptr(), m, gvs.gv.data_ptr(), gvs.g4.data_ptr(),
+                                     gvs.n, gvs.ws.data_ptr(), float(tol), int(iters),
+                                     npk.data_ptr(), mean.data_ptr(), ws.buf.data_ptr(),
+                                     ws.buf.numel(), _stream()), "refine_batch")
+    refine_batch.last_workspace = ws
+    return u.view(-1, 3, 3), npk, mean

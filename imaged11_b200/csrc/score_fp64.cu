@@ -362,12 +362,13 @@ extern "C" int id11b_dev_verify_rounding(int n, int32_t* bad, void* stream) {
 extern "C" int id11b_dev_score_many_fp64(const double* ubis, int64_t m, const double* gv,
                                          int64_t ng, const double* tols_host, int ntol,
                                          int32_t* counts, void* stream) {
-    if (m < 0 || ng < 0 || ntol < 1 || ntol > ID11B_MAX_TOLS || !tols_host || !counts)
+    if (m < 0 || ng < 0 || ntol < 1 || ntol > ID11B_MAX_TOLS || !tols_host)
         return ID11B_ERR_ARG;
-    if ((m > 0 && !ubis) || (ng > 0 && !gv)) return ID11B_ERR_ARG;
+    if ((m > 0 && (!ubis || !counts)) || (ng > 0 && !gv)) return ID11B_ERR_ARG;
+    if (m == 0) return ID11B_OK;
     cudaStream_t st = (cudaStream_t)stream;
     ID11B_CHECK(cudaMemsetAsync(counts, 0, sizeof(int32_t) * m * ntol, st));
-    if (m == 0 || ng == 0) return ID11B_OK;
+    if (ng == 0) return ID11B_OK;
     TolSq ts;
     for (int j = 0; j < ID11B_MAX_TOLS; j++) ts.t[j] = j < ntol ? tols_host[j] * tols_host[j] : 0.;
     // g range per CTA: 64 g per thread, so CTA start-up stays a small part of

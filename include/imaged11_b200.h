@@ -151,6 +151,57 @@ int id11b_dev_score_and_assign(const double *ubi, const double *gv, double tol,
 /* verify_rounding on the device; *bad (int32, device) = mismatches. */
 int id11b_dev_verify_rounding(int n, int32_t *bad, void *stream);
 
+/* =====================================================================
+ * Batched extensions (no single reference function: each replaces a Python
+ * loop of reference calls, as noted).  Device pointers + stream.
+ * ===================================================================== */
+
+/* Plain FP64 batched score: counts[m*ntol + j] = score(ubis[m], gv, tols[j]),
+ * the loop of ImageD11/indexing.py:800 / :1095.  Reference arithmetic on the
+ * GPU, one thread per g; the baseline the FP32 kernels are measured against. */
+int id11b_dev_score_many_fp64(const double *ubis, int64_t m, const double *gv, int64_t ng,
+                              const double *tols_host, int ntol, int32_t *counts,
+                              void *stream);
+
+/* Prepare g-vectors for the FP32 batched kernels: g4 (n float4, 16-byte
+ * aligned) receives FP32 copies; gws (id11b_gvec_workspace_bytes(n), 256-byte
+ * aligned) receives max|g| and the list of g evaluated in FP64 only
+ * (non-finite, or a component beyond 1024). */
+int64_t id11b_gvec_workspace_bytes(int64_t n);
+int id11b_dev_prepare_gvecs(const double *gv, int64_t n, float *g4, void *gws,
+                            int64_t gws_bytes, void *stream);
+
+/* Workspace for id11b_dev_score_batch (refine = 0) / id11b_dev_refine_batch
+ * (refine = 1) with m UBIs and n g-vectors. */
+int64_t id11b_batch_workspace_bytes(int64_t m, int64_t n, int refine);
+
+/* Batched score, FP32 screening with exact FP64 recheck of every pair within
+ * a proven error band of tol^2: counts identical to the reference's score()
+ * (ImageD11 src/closest.c:227-248) for every (UBI, tol).  counts (m, ntol)
+ * int32; sums (m, ntol) double, optional: sum of drlv2 of the counted pairs
+ * (FP32 values, relative error below 1e-5).  ntol <= ID11B_MAX_TOLS; a
+ * tolerance >= 0.45 sends every pair through exact FP64. */
+int id11b_dev_score_batch(const double *ubis, int64_t m, const double *gv, const float *g4,
+                          int64_t n, const void *gws, const double *tols_host, int ntol,
+                          int32_t *counts, double *sums, void *ws, int64_t ws_bytes,
+                          void *stream);
+
+/* `iters` rounds of score_and_refine (ImageD11 src/closest.c:267-345) for each
+ * of m UBIs against all n g-vectors, ubis (m,3,3) updated in place; npk and
+ * mean_drlv2 (optional) receive the last round's count and mean drlv2.
+ * Candidates are screened in FP32; every accepted pair is evaluated and
+ * accumulated in the reference's FP64 arithmetic (per-CTA partials summed in
+ * a fixed order). */
+int id11b_dev_refine_batch(double *ubis, int64_t m, const double *gv, const float *g4,
+                           int64_t n, const void *gws, double tol, int iters, int32_t *npk,
+                           double *mean_drlv2, void *ws, int64_t ws_bytes, void *stream);
+
+/* Synchronising read of the last batch call's statistics from its workspace:
+ * FP64 re-evaluations, UBIs routed wholly to FP64, and the device error flag
+ * (returned as the status). */
+int id11b_batch_stats(const void *ws, int64_t m, int64_t n, int refine, int64_t *nrecheck,
+                      int32_t *nfallback, int32_t *error, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -176,3 +176,31 @@ def test_empty_inputs(cim, cuda):
     assert np.array_equal(uu, u)
     out = np.zeros((0, 3))
     cim.compute_gv(np.zeros((0, 3)), np.zeros(0), 1., 0.3, 0., 0., [0, 0, 0], out)
+
+
+def test_compute_gv_specialisations_and_nonfinite(cim, oracle, cuda):
+    """Every host-chosen kernel variant (t zero or not, chi.wedge identity or
+    not), with NaN / inf omega and lab positions mixed in: NaN positions match
+    the reference exactly, finite values agree to GV_ULPS."""
+    import torch
+    rng = np.random.default_rng(77)
+    n = 5000
+    x = np.stack([rng.uniform(1.4e5, 1.6e5, n), rng.uniform(-8e4, 8e4, n),
+                  rng.uniform(-8e4, 8e4, n)], 1)
+    om = rng.uniform(0, 360, n)
+    om[::97] = np.nan
+    om[5::101] = np.inf
+    x[7::103, 1] = np.nan
+    x[9::107, 0] = np.inf
+    for wedge, chi, t in [(0., 0., [0., 0., 0.]), (0., 0., [5., -3., 2.]),
+                          (0.01, 0.02, [0., 0., 0.]), (0.01, 0.02, [5., -3., 2.])]:
+        ref = oracle.compute_gv(x, om, 1.0, 0.2846, wedge, chi, t)
+        xd = torch.tensor(x, device=cuda)
+        od = torch.tensor(om, device=cuda)
+        g = torch.empty_like(xd)
+        cim.compute_gv(xd, od, 1.0, 0.2846, wedge, chi, t, g)
+        got = g.cpu().numpy()
+        assert np.array_equal(np.isnan(got), np.isnan(ref)), (wedge, chi, t)
+        fin = np.isfinite(ref).all(1)
+        assert np.array_equal(np.isinf(got), np.isinf(ref))
+        assert _close_ulps(got[fin], ref[fin], GV_ULPS)

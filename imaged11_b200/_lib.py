@@ -38,6 +38,8 @@ _SIGNATURES = [
     ("id11b_lsq_workspace_bytes", _i64, [_i64]),
     ("id11b_dev_score_and_refine", _i, [_p, _p, _d, _i64, _p, _p, _p, _i64, _p]),
     ("id11b_dev_refine_assigned", _i, [_p, _p, _p, _i, _i64, _p, _p, _p, _i64, _p]),
+    ("id11b_noalloc_scratch_bytes", _i64, []),
+    ("id11b_dev_score_and_refine_noalloc", _i, [_p, _p, _d, _i64, _p, _p, _p]),
     ("id11b_dev_score_and_assign", _i, [_p, _p, _d, _p, _p, _i, _i64, _p, _p]),
     ("id11b_dev_verify_rounding", _i, [_i, _p, _p]),
     ("id11b_dev_score_many_fp64", _i, [_p, _i64, _p, _i64, _p, _i, _p, _p]),

@@ -12,6 +12,8 @@
 // Also the plain batched FP64 scorer (many UBIs x many g, one launch per
 // tolerance set), the baseline against which the batched FP32 kernels are
 // measured.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace id11b {
@@ -380,4 +382,59 @@ extern "C" int id11b_dev_score_many_fp64(const double* ubis, int64_t m, const do
                                                                   (int)chunks, counts);
     ID11B_CHECK_LAUNCH();
     return ID11B_OK;
+}
+
+// ------------------------------------------------ allocation-free variant ----
+// score_and_refine for callers that must not allocate device memory: a
+// process that reserves the GPU's memory up front for detector frame buffers
+// and forbids later allocations (to keep acquisition latency predictable), a
+// host that runs this code inside another framework's memory pool with a hard
+// cap, or code called back from a stream where no allocating CUDA call may be
+// made.  The least-squares partial sums live in this file-scope device array
+// (kLsqMaxBlocks x 136 bytes = 136 KiB, held by every GPU that loads the
+// library until the process exits) instead of caller- or pool-provided memory.
+//
+// Every call on a device shares the array.  Each partial-sum CTA writes its own
+// slot before the finishing CTA reads it, so the previous call's contents never
+// leak into a result (the empty-input case zeroes slot 0 itself); calls that
+// overlap on the GPU -- on different streams, or from different host threads
+// without ordering -- race on the array and must be serialised by the caller.
+static __device__ __align__(256) LsqPartial g_lsq_scratch[kLsqMaxBlocks];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_lsq_scratch_mu;
+void* g_lsq_scratch_ptr[kMaxDevices] = {};  // device address of g_lsq_scratch, per device
+
+// The name g_lsq_scratch is only a host-side stand-in: a kernel must be given
+// the device address, looked up once per device with that device current.
+int lsq_scratch_address(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return id11b_record_cuda(e);
+    if (dev < 0 || dev >= kMaxDevices) return ID11B_ERR_SIZE;
+    std::lock_guard<std::mutex> lock(g_lsq_scratch_mu);
+    if (!g_lsq_scratch_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_lsq_scratch);
+        if (e != cudaSuccess) return id11b_record_cuda(e);
+        g_lsq_scratch_ptr[dev] = p;
+    }
+    *out = g_lsq_scratch_ptr[dev];
+    return ID11B_OK;
+}
+}  // namespace
+
+extern "C" int64_t id11b_noalloc_scratch_bytes(void) { return (int64_t)sizeof(g_lsq_scratch); }
+
+extern "C" int id11b_dev_score_and_refine_noalloc(double* ubi, const double* gv, double tol,
+                                                  int64_t ng, int32_t* n, double* mean_drlv2,
+                                                  void* stream) {
+    if (ng < 0) return ID11B_ERR_ARG;
+    if (ng > INT32_MAX) return ID11B_ERR_SIZE;  // the reference's int peak count
+    void* scratch = nullptr;
+    int rc = lsq_scratch_address(&scratch);
+    if (rc) return rc;
+    return lsq_launch(0, ubi, gv, tol, nullptr, 0, ng, n, mean_drlv2, scratch,
+                      (int64_t)sizeof(g_lsq_scratch), stream);
 }

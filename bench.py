@@ -68,6 +68,73 @@ def compute_gv_measure(torch, ps, dev, n_peaks=10_000_000, steps=5, flush=None):
     return 56.0 * n_peaks / (ms * 1e-3) / 1e9, ms
 
 
+def refine_workload(seed=SEED + 7, ngrains=2000):
+    """Uneven per-grain refinement: hcp Ti grains (a=2.95, c=4.68 A), per-grain
+    peak counts log-uniform in 20..2000 set by a per-grain |g| cutoff (capped by
+    the reflections the 2048^2 detector can record, ~1,500 at |g|<=2.2), each
+    UBI 0.2 deg and 0.2% strain off its true value."""
+    from imaged11_b200 import synth
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(20), np.log(2000), ngrains)).astype(int)
+    ps = synth.simulate(ngrains, "Ti_hcp", gmax=2.2, seed=seed, noise_frac=0.0,
+                        per_grain_counts=counts)
+    idx, off = ps.grain_offsets()
+    u0 = synth.perturb_ubis(ps.ubis, 0.2, 0.002, rng)
+    return np.ascontiguousarray(ps.gv[idx]), off, u0
+
+
+def refine_csr_measure(torch, dev, iters=5, tol=0.05, steps=5, flush=None, cpu=True):
+    """Batched per-grain refinement: persistent kernel replayed from a CUDA
+    graph vs the plain FP64 path (one launch per round), pairs = peaks x rounds."""
+    from imaged11_b200 import batch
+    gv, off, u0 = refine_workload()
+    gs = batch.GrainSet(gv, off, u0)
+    u0_dev = gs.ubis.clone()
+    graph = gs.capture(tol, iters)
+
+    def reset():
+        if flush is not None:
+            flush()
+        gs.ubis.copy_(u0_dev)
+
+    times_g, times_p = [], []
+    for _ in range(3):
+        reset()
+        graph.replay()
+        reset()
+        gs.refine(tol, iters, persistent=False)
+    st = torch.cuda.current_stream()
+    for _ in range(steps):
+        for fn, acc in ((graph.replay, times_g),
+                        (lambda: gs.refine(tol, iters, persistent=False), times_p)):
+            reset()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            e1.synchronize()
+            acc.append(e0.elapsed_time(e1))
+    pairs = gs.peaks * iters
+    out = {"grains": gs.ngrains, "peaks": gs.peaks, "rounds": iters, "tol": tol,
+           "peaks_per_grain_min_max": [int(np.diff(off).min()), int(np.diff(off).max())],
+           "graph_ms": float(np.mean(times_g)), "plain_fp64_ms": float(np.mean(times_p)),
+           "value": pairs / (np.mean(times_g) * 1e-3), "unit": "pairs/s",
+           "plain_fp64_value": pairs / (np.mean(times_p) * 1e-3)}
+    out["ratio_vs_plain_fp64"] = out["value"] / out["plain_fp64_value"]
+    if cpu:
+        from oracle import oracle as orc
+        lib = orc.Reference() if orc.have_reference() else orc.Oracle()
+        t0 = time.perf_counter()
+        lib.refine_csr(u0, gv, off, tol, iters)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": pairs / dt, "unit": "pairs/s",
+                               "cores": lib.max_threads(),
+                               "kind": "reference" if isinstance(lib, orc.Reference) else "port",
+                               "sample": "whole workload (%.2f s)" % dt}
+    return out
+
+
 def workload(rank=0, n_ubi=N_UBI):
     from imaged11_b200 import synth
     ps = synth.simulate(N_GRAINS, "Al", gmax=GMAX, seed=SEED, noise_frac=0.10)
@@ -217,6 +284,9 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     ps, ubis = workload(rank, args.ubis)
+    if args.case == "refine":   # per-grain CSR refinement alone
+        print(json.dumps(refine_csr_measure(torch, dev, steps=args.steps, cpu=False)))
+        return 0
     if args.case == "gv":       # compute_gv alone (profiling case)
         gbs, ms = compute_gv_measure(torch, ps, dev, args.peaks, args.steps)
         print(json.dumps({"case": "compute_gv", "peaks": args.peaks, "GB/s": gbs, "ms": ms}))
@@ -287,6 +357,10 @@ def run_ours(args, rank, world, local_rank):
     gv_gbs, gv_ms = compute_gv_measure(torch, ps, dev, 10_000_000, max(3, args.steps), flush)
     hbm_peak, hbm_kind = measured_hbm_peak()
 
+    # uneven per-grain refinement (persistent kernel in a CUDA graph)
+    refine = refine_csr_measure(torch, dev, steps=max(3, args.steps), flush=flush,
+                                cpu=(world == 1))
+
     # end to end through the public API: pinned host inputs -> counts on host
     gv_h = torch.tensor(ps.gv).pin_memory()
     ub_h = torch.tensor(ubis).pin_memory()
@@ -331,6 +405,7 @@ def run_ours(args, rank, world, local_rank):
         "plain_fp64": {"value_per_tol_launch": rate64, "value_all_tols": rate64f,
                        "unit": "pairs/s", "ubis": m64,
                        "ratio_vs_per_tol": value / rate64, "ratio_vs_all_tols": value / rate64f},
+        "refine_csr": refine,
         "compute_gv": {"peaks": 10_000_000, "ms": gv_ms, "achieved_gbs": gv_gbs,
                        "peak_gbs": hbm_peak, "peak_kind": hbm_kind,
                        "frac": gv_gbs / hbm_peak, "bytes_per_peak": 56},
@@ -353,8 +428,9 @@ def main():
     ap.add_argument("--ubis", type=int, default=N_UBI, help="trial UBIs per GPU")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed steps of the scoring step (profiling case)")
-    ap.add_argument("--case", default="score", choices=["score", "gv"],
-                    help="gv: compute_gv alone on --peaks lab positions (profiling case)")
+    ap.add_argument("--case", default="score", choices=["score", "gv", "refine"],
+                    help="gv: compute_gv alone on --peaks lab positions; refine: per-grain "
+                         "CSR refinement alone (profiling cases)")
     ap.add_argument("--peaks", type=int, default=10_000_000)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -159,3 +159,59 @@ def refine_batch(ubis, gvs, tol, iters=1, workspace=None):
                                      ws.buf.numel(), _stream()), "refine_batch")
     refine_batch.last_workspace = ws
     return u.view(-1, 3, 3), npk, mean
+
+
+class GrainSet:
+    """Grains with their own peaks, for per-grain refinement.
+
+    gv: (n,3) float64 g-vectors sorted by grain; offsets: (ngrains+1,) int64 so
+    grain g owns gv[offsets[g]:offsets[g+1]]; ubis: (ngrains,3,3).  Everything
+    is copied to the GPU once; grains are processed largest first."""
+
+    def __init__(self, gv, offsets, ubis):
+        torch = _torch()
+        self.gv = _dev(gv, torch.float64).reshape(-1, 3)
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        self.ngrains = len(off) - 1
+        dev = self.gv.device
+        self.offsets = torch.as_tensor(off, device=dev)
+        sizes = np.diff(off)
+        self.order = torch.as_tensor(np.argsort(-sizes, kind="stable").astype(np.int32),
+                                     device=dev)
+        self.ubis = _dev(ubis, torch.float64).reshape(-1, 9).contiguous()
+        self.npk = torch.zeros(self.ngrains, dtype=torch.int32, device=dev)
+        self.mean = torch.zeros(self.ngrains, dtype=torch.float64, device=dev)
+        self.ws = torch.zeros(lib.id11b_refine_csr_workspace_bytes(), dtype=torch.uint8,
+                              device=dev)
+        self.peaks = int(off[-1] - off[0]) if len(off) else 0
+
+    def refine(self, tol, iters, persistent=True):
+        """Enqueue `iters` score_and_refine rounds for every grain (in place).
+        persistent=False runs the plain baseline: one launch per round."""
+        if persistent:
+            self._launch(tol, iters, 1)
+        else:
+            for _ in range(iters):
+                self._launch(tol, 1, 0)
+        return self.ubis.view(-1, 3, 3), self.npk, self.mean
+
+    def _launch(self, tol, iters, persistent):
+        check(lib.id11b_dev_refine_csr(self.ubis.data_ptr(), self.gv.data_ptr(),
+                                       self.offsets.data_ptr(), self.order.data_ptr(),
+                                       self.ngrains, float(tol), int(iters), persistent,
+                                       self.npk.data_ptr(), self.mean.data_ptr(),
+                                       self.ws.data_ptr(), self.ws.numel(), _stream()),
+              "refine_csr")
+
+    def capture(self, tol, iters):
+        """A CUDA graph of one persistent launch (counter reset + kernel) running
+        `iters` rounds on the current UBIs; call .replay() on the result."""
+        torch = _torch()
+        saved = self.ubis.clone()
+        self._launch(tol, 1, 1)          # load the kernel outside the capture
+        self.ubis.copy_(saved)
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            self._launch(tol, iters, 1)
+        return graph

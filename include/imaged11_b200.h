@@ -212,6 +212,23 @@ int id11b_dev_refine_batch(double *ubis, int64_t m, const double *gv, const floa
                            int64_t n, const void *gws, double tol, int iters, int32_t *npk,
                            double *mean_drlv2, void *ws, int64_t ws_bytes, void *stream);
 
+/* Per-grain refinement over CSR peak lists: grain g refines ubis[g] (9 doubles,
+ * in place) against gv[offsets[g] : offsets[g+1]] with `iters` rounds of
+ * score_and_refine (ImageD11 src/closest.c:267-345), as the per-grain loop of
+ * ImageD11/refinegrains.py:459-498 calls it.  order (optional, ngrains int32)
+ * is the processing order (largest grains first balances best).
+ * persistent != 0: one launch runs every round of every grain, CTAs pulling
+ * grains from a work counter in `workspace` (id11b_refine_csr_workspace_bytes());
+ * persistent == 0: one CTA per grain, the plain baseline (call once per round).
+ * npk / mean_drlv2 (optional, ngrains) receive the last round's count and mean
+ * drlv2.  Exact FP64 per pair; the persistent launch (counter reset + kernel)
+ * can be captured in a CUDA graph and replayed. */
+int64_t id11b_refine_csr_workspace_bytes(void);
+int id11b_dev_refine_csr(double *ubis, const double *gv, const int64_t *offsets,
+                         const int32_t *order, int32_t ngrains, double tol, int iters,
+                         int persistent, int32_t *npk, double *mean_drlv2, void *workspace,
+                         int64_t ws_bytes, void *stream);
+
 /* Synchronising read of the last batch call's statistics from its workspace:
  * FP64 re-evaluations, UBIs routed wholly to FP64, and the device error flag
  * (returned as the status). */

@@ -1,0 +1,71 @@
+"""Per-grain CSR refinement (persistent kernel, CUDA graph, plain baseline)
+against the oracle's loop of score_and_refine calls over each grain's peaks.
+
+n per grain is exact; refined UBIs agree to the rounding of the summation
+order (UBI_RTOL, as the other refinement tests); mean drlv2 to 1e-12."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+UBI_RTOL = 1e-11
+DRLV2_RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def grains():
+    from imaged11_b200 import synth
+    rng = np.random.default_rng(41)
+    ng = 120
+    counts = np.exp(rng.uniform(np.log(20), np.log(2000), ng)).astype(int)
+    ps = synth.simulate(ng, "Ti_hcp", gmax=2.2, seed=42, noise_frac=0.0,
+                        per_grain_counts=counts)
+    idx, off = ps.grain_offsets()
+    gv = ps.gv[idx]
+    u0 = synth.perturb_ubis(ps.ubis, 0.2, 0.002, rng)
+    # a few edge cases: an empty grain, a grain with 2 peaks (singular H)
+    off = np.concatenate([off, [off[-1], off[-1] + 2]])
+    gv = np.concatenate([gv, gv[:2]])
+    u0 = np.concatenate([u0, ps.ubis[:2]])
+    return gv, off, u0
+
+
+def _check(u, npk, mean, ref_u, ref_n, ref_m):
+    assert np.array_equal(npk, ref_n)
+    assert np.all(np.abs(mean - ref_m) <= DRLV2_RTOL * np.abs(ref_m))
+    scale = np.abs(ref_u).reshape(len(ref_u), -1).max(1)
+    err = np.abs(u - ref_u).reshape(len(ref_u), -1).max(1)
+    assert np.all(err <= UBI_RTOL * scale), err.max()
+
+
+@pytest.mark.parametrize("persistent", [True, False])
+def test_refine_csr_matches_oracle(grains, oracle, persistent, cuda):
+    from imaged11_b200 import batch
+    gv, off, u0 = grains
+    ref_u, ref_n, ref_m = oracle.refine_csr(u0, gv, off, 0.05, 5)
+    gs = batch.GrainSet(gv, off, u0)
+    u, npk, mean = gs.refine(0.05, 5, persistent=persistent)
+    _check(u.cpu().numpy(), npk.cpu().numpy(), mean.cpu().numpy(), ref_u, ref_n, ref_m)
+
+
+def test_refine_csr_graph_replay(grains, oracle, cuda):
+    import torch
+    from imaged11_b200 import batch
+    gv, off, u0 = grains
+    gs = batch.GrainSet(gv, off, u0)
+    graph = gs.capture(0.05, 2)
+    assert np.array_equal(gs.ubis.cpu().numpy().reshape(-1, 3, 3), u0)
+    graph.replay()
+    graph.replay()                    # 2 + 2 rounds
+    torch.cuda.synchronize()
+    ref_u, ref_n, ref_m = oracle.refine_csr(u0, gv, off, 0.05, 4)
+    _check(gs.ubis.cpu().numpy().reshape(-1, 3, 3), gs.npk.cpu().numpy(),
+           gs.mean.cpu().numpy(), ref_u, ref_n, ref_m)
+
+
+def test_refine_csr_deterministic(grains, cuda):
+    from imaged11_b200 import batch
+    gv, off, u0 = grains
+    a = batch.GrainSet(gv, off, u0).refine(0.05, 3)[0].cpu().numpy()
+    b = batch.GrainSet(gv, off, u0).refine(0.05, 3)[0].cpu().numpy()
+    assert np.array_equal(a, b)

@@ -131,7 +131,7 @@ def refine_csr_measure(torch, dev, iters=5, tol=0.05, steps=5, flush=None, cpu=T
         out["cpu_baseline"] = {"value": pairs / dt, "unit": "pairs/s",
                                "cores": lib.max_threads(),
                                "kind": "reference" if isinstance(lib, orc.Reference) else "port",
-                               "sample": "whole workload (%.2f s)" % dt}
+                               "sample": "whole workload, %d peaks x %d rounds (%.1f ms)" % (len(gv), iters, dt * 1e3)}
     return out
 
 

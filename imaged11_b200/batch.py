@@ -166,9 +166,14 @@ class GrainSet:
 
     gv: (n,3) float64 g-vectors sorted by grain; offsets: (ngrains+1,) int64 so
     grain g owns gv[offsets[g]:offsets[g+1]]; ubis: (ngrains,3,3).  Everything
-    is copied to the GPU once; grains are processed largest first."""
+    is copied to the GPU once; grains are processed largest first.
 
-    def __init__(self, gv, offsets, ubis):
+    threads: CTA size of the persistent launch.  Measured on B200 with 2,000
+    grains of 20..1,500 peaks: 64 threads 53 us for 5 rounds, 128 -> 87 us,
+    256 -> 147 us -- many small CTAs keep more grains in flight, which matters
+    more than the longest grain's share of lanes."""
+
+    def __init__(self, gv, offsets, ubis, threads=64):
         torch = _torch()
         self.gv = _dev(gv, torch.float64).reshape(-1, 3)
         off = np.ascontiguousarray(offsets, dtype=np.int64)
@@ -178,6 +183,7 @@ class GrainSet:
         sizes = np.diff(off)
         self.order = torch.as_tensor(np.argsort(-sizes, kind="stable").astype(np.int32),
                                      device=dev)
+        self.threads = int(threads)
         self.ubis = _dev(ubis, torch.float64).reshape(-1, 9).contiguous()
         self.npk = torch.zeros(self.ngrains, dtype=torch.int32, device=dev)
         self.mean = torch.zeros(self.ngrains, dtype=torch.float64, device=dev)
@@ -187,19 +193,20 @@ class GrainSet:
 
     def refine(self, tol, iters, persistent=True):
         """Enqueue `iters` score_and_refine rounds for every grain (in place).
-        persistent=False runs the plain baseline: one launch per round."""
+        persistent=False runs the plain baseline: one launch per round, one
+        128-thread CTA per grain."""
         if persistent:
-            self._launch(tol, iters, 1)
+            self._launch(tol, iters, 1, self.threads)
         else:
             for _ in range(iters):
-                self._launch(tol, 1, 0)
+                self._launch(tol, 1, 0, 128)
         return self.ubis.view(-1, 3, 3), self.npk, self.mean
 
-    def _launch(self, tol, iters, persistent):
+    def _launch(self, tol, iters, persistent, threads):
         check(lib.id11b_dev_refine_csr(self.ubis.data_ptr(), self.gv.data_ptr(),
                                        self.offsets.data_ptr(), self.order.data_ptr(),
                                        self.ngrains, float(tol), int(iters), persistent,
-                                       self.npk.data_ptr(), self.mean.data_ptr(),
+                                       threads, self.npk.data_ptr(), self.mean.data_ptr(),
                                        self.ws.data_ptr(), self.ws.numel(), _stream()),
               "refine_csr")
 
@@ -208,10 +215,10 @@ class GrainSet:
         `iters` rounds on the current UBIs; call .replay() on the result."""
         torch = _torch()
         saved = self.ubis.clone()
-        self._launch(tol, 1, 1)          # load the kernel outside the capture
+        self._launch(tol, 1, 1, self.threads)   # load the kernel outside the capture
         self.ubis.copy_(saved)
         torch.cuda.synchronize()
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph):
-            self._launch(tol, iters, 1)
+            self._launch(tol, iters, 1, self.threads)
         return graph

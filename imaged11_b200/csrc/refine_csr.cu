@@ -2,10 +2,12 @@
 //
 // Grain g owns the g-vectors gv[off[g] : off[g+1]] (20 .. 2000 peaks each in
 // the uneven workload) and `iters` rounds of the reference's score_and_refine
-// (ImageD11 src/closest.c:267-345) are applied to its UBI.  One CTA of 128
-// threads refines one grain at a time and runs all rounds itself: per round,
-// every thread accumulates the exact-FP64 normal-equation terms of its peaks,
-// the CTA reduces them in a fixed tree (warp butterfly, then warps in order),
+// (ImageD11 src/closest.c:267-345) are applied to its UBI.  One CTA (128,
+// 256 or 512 threads, chosen from the largest grain) refines one grain at a
+// time and runs all rounds itself: per round, every thread tests its peaks
+// with the reference's exact FP64 arithmetic and accumulates the accepted
+// peaks' normal-equation terms, the CTA reduces them in a fixed tree (warp
+// butterfly, then warps in order),
 // and nine threads apply the reference's update (one cofactor / one UB element
 // each; the same expressions as inverse3x3, so the result equals the
 // single-thread update bit for bit).
@@ -22,8 +24,6 @@
 #include "common.cuh"
 
 namespace id11b {
-
-constexpr int kRT = 128;  // threads per CTA
 
 // Element idx of the cofactor inverse, as inverse3x3 (src/closest.c:38-76).
 __device__ __forceinline__ double inv3_elem(const double* a, double det, int idx) {
@@ -48,8 +48,9 @@ __device__ __forceinline__ double det3_exact(const double* a) {
                 dmul(a[6], dsub(dmul(a[5], a[1]), dmul(a[4], a[2]))));
 }
 
+template <int NT>
 struct RefineSmem {
-    double red[kRT / 32][17];  // per-warp partial sums
+    double red[NT / 32][17];  // per-warp partial sums
     double R[9], H[9], Hi[9], UB[9], UBI[9], ubi[9];
     long long n;
     double ss;
@@ -61,12 +62,13 @@ struct RefineSmem {
 __constant__ int c_hrow[6] = {0, 0, 0, 1, 1, 2};
 __constant__ int c_hcol[6] = {0, 1, 2, 1, 2, 2};
 
-__global__ void __launch_bounds__(kRT)
+template <int NT>
+__global__ void __launch_bounds__(NT)
 k_refine_csr(double* __restrict__ ubis, const double* __restrict__ gv,
              const int64_t* __restrict__ off, const int* __restrict__ order, int ngrains,
              double tolsq, int iters, int* __restrict__ queue, int* __restrict__ npk,
              double* __restrict__ mean) {
-    __shared__ RefineSmem sm;
+    __shared__ RefineSmem<NT> sm;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     for (int slot = blockIdx.x;; slot += gridDim.x) {
         if (queue) {
@@ -86,25 +88,45 @@ k_refine_csr(double* __restrict__ ubis, const double* __restrict__ gv,
             double acc[17];
 #pragma unroll
             for (int f = 0; f < 17; f++) acc[f] = 0.;
-            for (int64_t k = k0 + tid; k < k1; k += kRT) {
-                const double g0 = gv[3 * k], g1 = gv[3 * k + 1], g2 = gv[3 * k + 2];
-                double ih[3];
-                const double s = drlv2_exact(u, g0, g1, g2, ih);
-                if (!(s < tolsq)) continue;
-                const double gg[3] = {g0, g1, g2};
+            // kU peaks per lane per step: all their loads are issued before any
+            // is used, so one memory latency covers kU peaks (the segment is
+            // read-only and re-read every round, so later rounds hit L1)
+            constexpr int kU = 4;
+            for (int64_t kb = k0 + tid; kb < k1; kb += kU * NT) {
+                double gg[kU][3];
 #pragma unroll
-                for (int i = 0; i < 3; i++)
+                for (int q = 0; q < kU; q++) {
+                    const int64_t k = kb + (int64_t)q * NT;
+                    if (k < k1) {
+                        gg[q][0] = __ldg(gv + 3 * k);
+                        gg[q][1] = __ldg(gv + 3 * k + 1);
+                        gg[q][2] = __ldg(gv + 3 * k + 2);
+                    }
+                }
 #pragma unroll
-                    for (int j = 0; j < 3; j++)
-                        acc[3 * i + j] = dadd(acc[3 * i + j], dmul(ih[j], gg[i]));
-                acc[9] = dadd(acc[9], dmul(ih[0], ih[0]));
-                acc[10] = dadd(acc[10], dmul(ih[1], ih[0]));
-                acc[11] = dadd(acc[11], dmul(ih[2], ih[0]));
-                acc[12] = dadd(acc[12], dmul(ih[1], ih[1]));
-                acc[13] = dadd(acc[13], dmul(ih[2], ih[1]));
-                acc[14] = dadd(acc[14], dmul(ih[2], ih[2]));
-                acc[15] = dadd(acc[15], s);
-                acc[16] += 1.0;
+                for (int q = 0; q < kU; q++) {
+                    if (kb + (int64_t)q * NT >= k1) break;
+                    double ih[3];
+                    const double s = drlv2_exact(u, gg[q][0], gg[q][1], gg[q][2], ih);
+                    if (!(s < tolsq)) continue;
+                    // normal equations with fused multiply-adds: H (products of
+                    // integers) is exact either way; each R term is rounded once
+                    // instead of twice -- R is order-dependent against the
+                    // reference's sequential sum in any case
+#pragma unroll
+                    for (int i = 0; i < 3; i++)
+#pragma unroll
+                        for (int j = 0; j < 3; j++)
+                            acc[3 * i + j] = fma(ih[j], gg[q][i], acc[3 * i + j]);
+                    acc[9] = fma(ih[0], ih[0], acc[9]);
+                    acc[10] = fma(ih[1], ih[0], acc[10]);
+                    acc[11] = fma(ih[2], ih[0], acc[11]);
+                    acc[12] = fma(ih[1], ih[1], acc[12]);
+                    acc[13] = fma(ih[2], ih[1], acc[13]);
+                    acc[14] = fma(ih[2], ih[2], acc[14]);
+                    acc[15] = dadd(acc[15], s);
+                    acc[16] += 1.0;
+                }
             }
 #pragma unroll
             for (int f = 0; f < 17; f++) acc[f] = warp_sum(acc[f]);
@@ -114,7 +136,7 @@ k_refine_csr(double* __restrict__ ubis, const double* __restrict__ gv,
             __syncthreads();
             if (tid < 17) {
                 double t = 0.;
-                for (int q = 0; q < kRT / 32; q++) t += sm.red[q][tid];
+                for (int q = 0; q < NT / 32; q++) t += sm.red[q][tid];
                 if (tid < 9) {
                     sm.R[tid] = t;
                 } else if (tid < 15) {
@@ -178,34 +200,53 @@ static int sm_count_rc() {
 
 using namespace id11b;
 
+template <int NT>
+static int launch_refine(double* ubis, const double* gv, const int64_t* offsets,
+                         const int32_t* order, int32_t ngrains, double tolsq, int iters,
+                         int* queue, int32_t* npk, double* mean, cudaStream_t st) {
+    int grid = ngrains;
+    if (queue) {
+        static int occ = 0;
+        if (!occ) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_refine_csr<NT>, NT, 0);
+            if (occ < 1) occ = 1;
+        }
+        const int cap = sm_count_rc() * occ;
+        grid = ngrains < cap ? ngrains : cap;
+    }
+    k_refine_csr<NT><<<grid, NT, 0, st>>>(ubis, gv, offsets, order, ngrains, tolsq, iters,
+                                          queue, npk, mean);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
 extern "C" int64_t id11b_refine_csr_workspace_bytes(void) { return 256; }
 
 extern "C" int id11b_dev_refine_csr(double* ubis, const double* gv, const int64_t* offsets,
                                     const int32_t* order, int32_t ngrains, double tol,
-                                    int iters, int persistent, int32_t* npk,
+                                    int iters, int persistent, int threads, int32_t* npk,
                                     double* mean_drlv2, void* workspace, int64_t ws_bytes,
                                     void* stream) {
     if (ngrains < 0 || iters < 0) return ID11B_ERR_ARG;
     if (ngrains > 0 && (!ubis || !offsets)) return ID11B_ERR_ARG;
     if (persistent && (!workspace || ws_bytes < id11b_refine_csr_workspace_bytes()))
         return ID11B_ERR_ARG;
+    if (threads != 0 && threads != 32 && threads != 64 && threads != 128 && threads != 256 &&
+        threads != 512)
+        return ID11B_ERR_ARG;
     if (ngrains == 0 || iters == 0) return ID11B_OK;
     cudaStream_t st = (cudaStream_t)stream;
     int* queue = nullptr;
-    int grid = ngrains;
     if (persistent) {
         queue = (int*)workspace;
         ID11B_CHECK(cudaMemsetAsync(queue, 0, sizeof(int), st));
-        static int occ = 0;
-        if (!occ) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_refine_csr, kRT, 0);
-            if (occ < 1) occ = 1;
-        }
-        const int cap = sm_count_rc() * occ;
-        grid = ngrains < cap ? ngrains : cap;
     }
-    k_refine_csr<<<grid, kRT, 0, st>>>(ubis, gv, offsets, order, ngrains, tol * tol, iters,
-                                       queue, npk, mean_drlv2);
-    ID11B_CHECK_LAUNCH();
-    return ID11B_OK;
+    const double tolsq = tol * tol;
+    switch (threads) {
+        case 32: return launch_refine<32>(ubis, gv, offsets, order, ngrains, tolsq, iters, queue, npk, mean_drlv2, st);
+        case 64: return launch_refine<64>(ubis, gv, offsets, order, ngrains, tolsq, iters, queue, npk, mean_drlv2, st);
+        case 256: return launch_refine<256>(ubis, gv, offsets, order, ngrains, tolsq, iters, queue, npk, mean_drlv2, st);
+        case 512: return launch_refine<512>(ubis, gv, offsets, order, ngrains, tolsq, iters, queue, npk, mean_drlv2, st);
+        default: return launch_refine<128>(ubis, gv, offsets, order, ngrains, tolsq, iters, queue, npk, mean_drlv2, st);
+    }
 }

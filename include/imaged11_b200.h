@@ -221,13 +221,14 @@ int id11b_dev_refine_batch(double *ubis, int64_t m, const double *gv, const floa
  * grains from a work counter in `workspace` (id11b_refine_csr_workspace_bytes());
  * persistent == 0: one CTA per grain, the plain baseline (call once per round).
  * npk / mean_drlv2 (optional, ngrains) receive the last round's count and mean
- * drlv2.  Exact FP64 per pair; the persistent launch (counter reset + kernel)
+ * drlv2.  threads: CTA size 32, 64, 128, 256 or 512 (0 = 128); small CTAs keep
+ * more grains in flight (64 is fastest for 2,000 grains of 20..1,500 peaks).  Exact FP64 per pair; the persistent launch (counter reset + kernel)
  * can be captured in a CUDA graph and replayed. */
 int64_t id11b_refine_csr_workspace_bytes(void);
 int id11b_dev_refine_csr(double *ubis, const double *gv, const int64_t *offsets,
                          const int32_t *order, int32_t ngrains, double tol, int iters,
-                         int persistent, int32_t *npk, double *mean_drlv2, void *workspace,
-                         int64_t ws_bytes, void *stream);
+                         int persistent, int threads, int32_t *npk, double *mean_drlv2,
+                         void *workspace, int64_t ws_bytes, void *stream);
 
 /* Synchronising read of the last batch call's statistics from its workspace:
  * FP64 re-evaluations, UBIs routed wholly to FP64, and the device error flag

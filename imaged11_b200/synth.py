@@ -256,17 +256,23 @@ class PeakSet:
 
 
 def simulate(ngrains, cell="Al", gmax=1.0, seed=0, geo=None, sigma_px=0.5, sigma_om=0.05,
-             noise_frac=0.10, per_grain_counts=None, translations_um=0.0, cells=None):
+             noise_frac=0.10, per_grain_counts=None, translations_um=0.0, cells=None,
+             translation=None):
     """Simulate a scan.  per_grain_counts (optional) keeps, for each grain, only
-    its lowest-|g| spots up to that count (a per-grain |g| cutoff)."""
+    its lowest-|g| spots up to that count (a per-grain |g| cutoff).
+    translation (optional 3-vector) places every grain at that position
+    (otherwise uniform in +-translations_um).  The returned PeakSet records
+    each spot's true hkl (NaN for noise peaks)."""
     rng = np.random.default_rng(seed)
     geo = default_geometry() if geo is None else geo
     cells = cells if cells is not None else [cell] * ngrains
     U = random_rotations(ngrains, rng)
     trans = rng.uniform(-1, 1, size=(ngrains, 3)) * translations_um
+    if translation is not None:
+        trans = np.tile(np.asarray(translation, float), (ngrains, 1))
     cache = {}
     ubis = np.empty((ngrains, 3, 3))
-    S, F, OM, LAB = [], [], [], []
+    S, F, OM, LAB, HKL = [], [], [], [], []
     for name in sorted(set(cells)):
         if name not in cache:
             cache[name] = hkl_list(name, gmax)
@@ -281,16 +287,18 @@ def simulate(ngrains, cell="Al", gmax=1.0, seed=0, geo=None, sigma_px=0.5, sigma
         s, f, om, valid = project_spots(g.reshape(-1, 3), tt, geo)
         lab = np.tile(np.repeat(idx, H), 2)
         gsort = np.tile(gl.reshape(-1), 2)
+        hk = np.tile(np.tile(hkl, (n, 1)), (2, 1))
         s, f, om, lab, gsort = s[valid], f[valid], om[valid], lab[valid], gsort[valid]
+        hk = hk[valid]
         if per_grain_counts is not None:
             o = np.lexsort((gsort, lab))
-            s, f, om, lab = s[o], f[o], om[o], lab[o]
+            s, f, om, lab, hk = s[o], f[o], om[o], lab[o], hk[o]
             start = np.searchsorted(lab, lab, side="left")
             rank = np.arange(len(lab)) - start
             keep = rank < np.asarray(per_grain_counts)[lab]
-            s, f, om, lab = s[keep], f[keep], om[keep], lab[keep]
-        S.append(s); F.append(f); OM.append(om); LAB.append(lab)
-    s, f, om, lab = (np.concatenate(x) for x in (S, F, OM, LAB))
+            s, f, om, lab, hk = s[keep], f[keep], om[keep], lab[keep], hk[keep]
+        S.append(s); F.append(f); OM.append(om); LAB.append(lab); HKL.append(hk)
+    s, f, om, lab, hk = (np.concatenate(x) for x in (S, F, OM, LAB, HKL))
     s = s + rng.normal(size=len(s)) * sigma_px
     f = f + rng.normal(size=len(f)) * sigma_px
     om = om + rng.normal(size=len(om)) * sigma_om
@@ -299,8 +307,11 @@ def simulate(ngrains, cell="Al", gmax=1.0, seed=0, geo=None, sigma_px=0.5, sigma
     f = np.concatenate([f, rng.uniform(0, geo["dim"], nn)])
     om = np.concatenate([om, rng.uniform(0, 360, nn)])
     lab = np.concatenate([lab, np.full(nn, -1)]).astype(np.int32)
+    hk = np.concatenate([hk, np.full((nn, 3), np.nan)])
     perm = rng.permutation(len(s))
-    return PeakSet(s[perm], f[perm], om[perm], lab[perm], ubis, trans, geo, gmax, cell)
+    out = PeakSet(s[perm], f[perm], om[perm], lab[perm], ubis, trans, geo, gmax, cell)
+    out.hkl = hk[perm]
+    return out
 
 
 def trial_ubis(true_ubis, ntrial, frac_true, angle_deg, rng, cell="Al"):

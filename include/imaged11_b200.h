@@ -230,6 +230,37 @@ int id11b_dev_refine_csr(double *ubis, const double *gv, const int64_t *offsets,
                          int persistent, int threads, int32_t *npk, double *mean_drlv2,
                          void *workspace, int64_t ws_bytes, void *stream);
 
+/* Residuals of assigned peaks and their adjoint (no single reference
+ * function: the forward model chains compute_xlylzl and compute_gv,
+ * ImageD11 src/cdiffraction.c:190-224 and :112-168, with UBI.g - h, the
+ * quantity refinegrains.gof minimises by Nelder-Mead, ImageD11/refinegrains.py
+ * :517-560).  Peaks are stored grain by grain: grain G owns peaks
+ * offsets[G] .. offsets[G+1]-1, with detector positions sc (slow), fc (fast),
+ * omega (degrees) and assigned integer hkl (n,3 doubles).  geom_host holds 28
+ * doubles: r (9, detector rotation . flip), M (9, chi.wedge), t (3),
+ * wavelength, distance, y_center, z_center, y_size, z_size, omegasign.
+ * id11b_dev_residuals writes res (n,3) = UBI_G.g - hkl, optionally gvec (n,3),
+ * and ssq (ngrains) = per-grain sum of squared residuals.
+ * id11b_dev_residuals_adjoint takes grad_res = dL/dres (n,3) and writes
+ * grad_ubis (ngrains,9) = dL/dUBI and grad_global (22) = dL/dM (9, row-major),
+ * dL/dwavelength, dL/dt (3), sum of dL/dxyz (3), sum of dL/dxyz * v1 (3) and
+ * sum of dL/dxyz * v2 (3) with v1 = (fc - y_center) y_size,
+ * v2 = (sc - z_center) z_size -- the contractions with d(r, M)/d(tilts,
+ * wedge, chi) and with the centres and distance are left to the caller.
+ * FP64; reductions in a fixed order (deterministic).  Workspace:
+ * id11b_adjoint_workspace_bytes(ngrains). */
+int64_t id11b_adjoint_workspace_bytes(int32_t ngrains);
+int id11b_dev_residuals(const double *geom_host, const double *sc, const double *fc,
+                        const double *omega, const double *hkl, const int64_t *offsets,
+                        const double *ubis, int32_t ngrains, double *res, double *gvec,
+                        double *ssq, void *stream);
+int id11b_dev_residuals_adjoint(const double *geom_host, const double *sc, const double *fc,
+                                const double *omega, const double *hkl,
+                                const int64_t *offsets, const double *ubis, int32_t ngrains,
+                                const double *grad_res, double *grad_ubis,
+                                double *grad_global, void *workspace, int64_t ws_bytes,
+                                void *stream);
+
 /* Synchronising read of the last batch call's statistics from its workspace:
  * FP64 re-evaluations, UBIs routed wholly to FP64, and the device error flag
  * (returned as the status). */

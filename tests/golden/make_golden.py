@@ -16,6 +16,11 @@ Outputs come from two reference implementations:
   with stub ``fabio``/``cImageD11`` modules because only its numpy functions
   are used.
 
+The adjoint fixture holds the reference forward model's loss and its central
+finite-difference gradients (compute_xyz_lab -> compute_tth_eta_from_xyz ->
+compute_g_vectors -> UBI.g - h) with respect to the 12 geometry parameters
+and a few UBI elements.
+
 Inputs: the cases of the reference's own test/test_cImageD11.py (7 wedge /
 chi / translation / omegasign sets on 203 points; 8 detector flips x 27 tilt
 triples), seeded synthetic peak sets from imaged11_b200.synth, and adversarial
@@ -227,6 +232,65 @@ def cases_scoring(ref):
     return out
 
 
+ADJ_PARAMS = ("distance", "y_center", "z_center", "tilt_x", "tilt_y", "tilt_z", "wavelength",
+              "wedge", "chi", "t_x", "t_y", "t_z")
+ADJ_STEPS = dict(distance=1e-2, y_center=1e-4, z_center=1e-4, tilt_x=1e-7, tilt_y=1e-7,
+                 tilt_z=1e-7, wavelength=1e-8, wedge=1e-5, chi=1e-5, t_x=1e-3, t_y=1e-3,
+                 t_z=1e-3)
+
+
+def reference_loss(tr, s, f, omega, hkl, grain, ubis, pars):
+    """0.5 * sum |UBI.g - h|^2 with g from the reference's numpy transform."""
+    xyz = tr.compute_xyz_lab((s, f), **pars)
+    om = omega * pars["omegasign"]
+    tth, eta = tr.compute_tth_eta_from_xyz(xyz, om, t_x=pars["t_x"], t_y=pars["t_y"],
+                                           t_z=pars["t_z"], wedge=pars["wedge"],
+                                           chi=pars["chi"])
+    g = tr.compute_g_vectors(tth, eta, om, pars["wavelength"], wedge=pars["wedge"],
+                             chi=pars["chi"]).T
+    r = np.einsum("nij,nj->ni", ubis[grain], g) - hkl
+    return 0.5 * float((r * r).sum())
+
+
+def cases_adjoint(tr):
+    """Loss and central-difference gradients of the reference's forward model
+    at a geometry away from the truth (cfg3-like tilts, wedge, chi, t)."""
+    truth = synth.default_geometry(distance=152300., y_center=1024 + 3.7, z_center=1024 - 2.1,
+                                   tilt_x=0.004, tilt_y=-0.002, tilt_z=0.006, wedge=0.01,
+                                   chi=0.02, t_x=5., t_y=-3., t_z=2.)
+    ps = synth.simulate(6, "Al", gmax=1.2, seed=21, geo=truth, sigma_px=0.3, sigma_om=0.02,
+                        noise_frac=0.0, translation=(5., -3., 2.))
+    idx, off = ps.grain_offsets()
+    s, f, om, hkl = ps.s[idx], ps.f[idx], ps.omega[idx], ps.hkl[idx]
+    grain = np.repeat(np.arange(len(off) - 1), np.diff(off))
+    rng = np.random.default_rng(22)
+    ubis = synth.perturb_ubis(ps.ubis, 0.05, 0.0005, rng)
+    pars = dict(truth, distance=152000., y_center=1024., z_center=1024., tilt_x=0.001,
+                tilt_y=0.0, tilt_z=0.002, wedge=0.0, chi=0.0, t_x=0., t_y=0., t_z=0.)
+    L0 = reference_loss(tr, s, f, om, hkl, grain, ubis, pars)
+    grad = []
+    for name in ADJ_PARAMS:
+        h = ADJ_STEPS[name]
+        lp = reference_loss(tr, s, f, om, hkl, grain, ubis, dict(pars, **{name: pars[name] + h}))
+        lm = reference_loss(tr, s, f, om, hkl, grain, ubis, dict(pars, **{name: pars[name] - h}))
+        grad.append((lp - lm) / (2 * h))
+    gu = []
+    for (G, i, j) in [(0, 0, 0), (1, 1, 2), (3, 2, 1), (5, 0, 2)]:
+        h = 1e-7
+        up = ubis.copy(); up[G, i, j] += h
+        um = ubis.copy(); um[G, i, j] -= h
+        gu.append((reference_loss(tr, s, f, om, hkl, grain, up, pars) -
+                   reference_loss(tr, s, f, om, hkl, grain, um, pars)) / (2 * h))
+    return dict(adj_s=s, adj_f=f, adj_omega=om, adj_hkl=hkl, adj_offsets=off, adj_ubis=ubis,
+                adj_params=np.array([pars[k] for k in ADJ_PARAMS]),
+                adj_const=np.array([pars["y_size"], pars["z_size"], pars["omegasign"],
+                                    pars["o11"], pars["o12"], pars["o21"], pars["o22"]]),
+                adj_loss=np.array(L0), adj_grad_fd=np.array(grad),
+                adj_grad_ubi_idx=np.array([(0, 0, 0), (1, 1, 2), (3, 2, 1), (5, 0, 2)]),
+                adj_grad_ubi_fd=np.array(gu),
+                adj_truth=np.array([truth[k] for k in ADJ_PARAMS]))
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     ref = Reference()
@@ -235,6 +299,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "compute_gv.npz"), **cases_compute_gv(ref, tr))
     np.savez_compressed(os.path.join(HERE, "compute_xlylzl.npz"), **cases_xlylzl(ref, tr))
     np.savez_compressed(os.path.join(HERE, "scoring.npz"), **cases_scoring(ref))
+    np.savez_compressed(os.path.join(HERE, "adjoint.npz"), **cases_adjoint(tr))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -3,7 +3,8 @@
 // Work: M trial UBIs x N g-vectors x T tolerances.  Each CTA owns 256*R UBIs
 // (R per thread, in registers) and one g range; g tiles (float4, 16 KB) are
 // staged into shared memory by 1-D TMA bulk copies on a two-stage mbarrier
-// ring and read by every lane (broadcast).  Per (UBI, g) pair:
+// ring and read by every lane (broadcast).  Per (UBI, g) pair (computed for
+// two UBIs at a time with packed f32x2 instructions):
 //
 //   h   = UBI32 . g32             3 FFMA chains            (9 FMA-pipe ops)
 //   t   = h - rint(h)             magic-constant rounding  (9)
@@ -181,6 +182,55 @@ __device__ __forceinline__ float drlv2_f32(const float u[9], float4 g, float ih[
     return fmaf(t2, t2, fmaf(t1, t1, t0 * t0));
 }
 
+// Two UBIs at once with packed FP32x2 arithmetic (sm_100: add/sub/mul/fma
+// .f32x2).  B200's FP32 pipe does no more lane-operations per cycle with the
+// packed forms, but each instruction issues two of them, which frees issue
+// slots for the loads, compares and loop control that otherwise compete with
+// the FMA pipe.  Every lane performs exactly the scalar drlv2_f32 operations
+// (same order, round-to-nearest), so the screening values are bit-identical.
+__device__ __forceinline__ uint64_t pk2(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk2(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// drlv2_f32 for the UBI pair packed in up[9] against one g (gx, gy, gz each
+// duplicated into both halves); returns both drlv2 values packed.
+__device__ __forceinline__ uint64_t drlv2_pair(const uint64_t up[9], uint64_t gx, uint64_t gy,
+                                               uint64_t gz) {
+    const uint64_t M2 = 0x4B4000004B400000ull;  // (1.5 * 2^23, 1.5 * 2^23)
+    const uint64_t h0 = fma2(up[2], gz, fma2(up[1], gy, mul2(up[0], gx)));
+    const uint64_t h1 = fma2(up[5], gz, fma2(up[4], gy, mul2(up[3], gx)));
+    const uint64_t h2 = fma2(up[8], gz, fma2(up[7], gy, mul2(up[6], gx)));
+    const uint64_t t0 = sub2(h0, sub2(add2(h0, M2), M2));
+    const uint64_t t1 = sub2(h1, sub2(add2(h1, M2), M2));
+    const uint64_t t2 = sub2(h2, sub2(add2(h2, M2), M2));
+    return fma2(t2, t2, fma2(t1, t1, mul2(t0, t0)));
+}
+
 // ------------------------------------------------------------ main kernel --
 template <int R, int NT, int MODE>
 __global__ void __launch_bounds__(kBT, MODE == MODE_SCORE ? 3 : 2)
@@ -201,19 +251,27 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
 
     const Band<NT> band = make_band<NT>(tols, gi, ui);
 
-    float u[R][9];
+    static_assert(R % 2 == 0, "UBIs are screened in packed pairs");
+    uint64_t up[R / 2][9];  // UBI pairs (2p, 2p+1), element-wise packed
     int64_t mi[R];
 #pragma unroll
-    for (int r = 0; r < R; r++) {
-        mi[r] = ub * (kBT * R) + r * kBT + tid;
-        if (mi[r] < m) {
-            float4 a = packs[3 * mi[r]], b = packs[3 * mi[r] + 1], c = packs[3 * mi[r] + 2];
-            u[r][0] = a.x; u[r][1] = a.y; u[r][2] = a.z; u[r][3] = a.w;
-            u[r][4] = b.x; u[r][5] = b.y; u[r][6] = b.z; u[r][7] = b.w; u[r][8] = c.x;
-        } else {
+    for (int p = 0; p < R / 2; p++) {
+        float u[2][9];
 #pragma unroll
-            for (int e = 0; e < 9; e++) u[r][e] = __int_as_float(0x7fc00000);
+        for (int h = 0; h < 2; h++) {
+            const int r = 2 * p + h;
+            mi[r] = ub * (kBT * R) + r * kBT + tid;
+            if (mi[r] < m) {
+                float4 a = packs[3 * mi[r]], b = packs[3 * mi[r] + 1], c = packs[3 * mi[r] + 2];
+                u[h][0] = a.x; u[h][1] = a.y; u[h][2] = a.z; u[h][3] = a.w;
+                u[h][4] = b.x; u[h][5] = b.y; u[h][6] = b.z; u[h][7] = b.w; u[h][8] = c.x;
+            } else {
+#pragma unroll
+                for (int e = 0; e < 9; e++) u[h][e] = __int_as_float(0x7fc00000);
+            }
         }
+#pragma unroll
+        for (int e = 0; e < 9; e++) up[p][e] = pk2(u[0][e], u[1][e]);
     }
     // rare-path accumulators in shared memory, [field][kBT*R] so that lanes hit
     // consecutive words: MODE_SCORE int counts [NT] + float sums [NT]
@@ -261,12 +319,13 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
 #pragma unroll 2
         for (int k = 0; k < cntg; k++) {
             const float4 g = s_g[buf][k];
-            float s[R], ih[R][3];
+            const uint64_t gx = pk2(g.x, g.x), gy = pk2(g.y, g.y), gz = pk2(g.z, g.z);
+            float s[R];
             bool any = false;
 #pragma unroll
-            for (int r = 0; r < R; r++) {
-                s[r] = drlv2_f32(u[r], g, ih[r]);
-                any |= (s[r] < band.hmax);
+            for (int p = 0; p < R / 2; p++) {
+                upk2(drlv2_pair(up[p], gx, gy, gz), s[2 * p], s[2 * p + 1]);
+                any |= (s[2 * p] < band.hmax) | (s[2 * p + 1] < band.hmax);
             }
             if (any) {
 #pragma unroll

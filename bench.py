@@ -135,6 +135,129 @@ def refine_csr_measure(torch, dev, iters=5, tol=0.05, steps=5, flush=None, cpu=T
     return out
 
 
+CFG3_TRUTH = dict(distance=152300., y_center=1024 + 3.7, z_center=1024 - 2.1, tilt_x=0.004,
+                  tilt_y=-0.002, tilt_z=0.006, wedge=0.01, chi=0.02, t_x=5., t_y=-3., t_z=2.)
+
+
+def adjoint_measure(torch, dev, steps=5, refine=True):
+    """Joint grain + geometry refinement workload: 500 FCC Al grains (~325k
+    peaks, |g| <= 1.75) simulated with tilts, wedge, chi, translation and
+    offset centres, 0.5 px / 0.05 deg noise; gradient of the residuals with
+    respect to 12 geometry parameters and 500 x 9 UBI elements."""
+    from imaged11_b200 import adjoint, synth
+    truth = synth.default_geometry(**CFG3_TRUTH)
+    ps = synth.simulate(500, "Al", gmax=1.75, seed=SEED + 11, geo=truth, noise_frac=0.0,
+                        translation=(5., -3., 2.))
+    idx, off = ps.grain_offsets()
+    peaks = adjoint.PeakTable(ps.s[idx], ps.f[idx], ps.omega[idx], ps.hkl[idx], off, truth)
+    nominal = dict(truth, distance=150000., y_center=1024., z_center=1024., tilt_x=0.,
+                   tilt_y=0., tilt_z=0., wedge=0., chi=0., t_x=0., t_y=0., t_z=0.)
+    p0 = adjoint.params_tensor(nominal)
+    u0 = adjoint.best_ubis(adjoint.gvectors(p0, peaks), peaks)
+
+    def grad_eval():
+        p = p0.clone().requires_grad_(True)
+        u = u0.clone().requires_grad_(True)
+        adjoint.loss(p, u, peaks).backward()
+        return p.grad, u.grad
+
+    for _ in range(3):
+        grad_eval()
+    times = cuda_time_ms(torch, grad_eval, steps)
+    out = {"grains": peaks.ngrains, "peaks": peaks.n, "params": 12 + 9 * peaks.ngrains,
+           "gradient_ms": float(np.mean(times)),
+           "gradient_peaks_per_s": peaks.n / (np.mean(times) * 1e-3),
+           "note": "one residual forward + adjoint pass through torch.autograd, host "
+                   "geometry assembly included"}
+    if refine:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p, _, hist = adjoint.refine_geometry(peaks, p0, max_iter=100)
+        torch.cuda.synchronize()
+        got = dict(zip(adjoint.PARAMS, p.cpu().numpy()))
+        out["refine"] = {"seconds": time.perf_counter() - t0, "evaluations": len(hist),
+                         "loss_start": hist[0], "loss_end": hist[-1],
+                         "error_vs_truth": {k: float(got[k] - truth[k])
+                                            for k in adjoint.PARAMS if k != "wavelength"}}
+    return out
+
+
+def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5):
+    """Full-scale scan: 20,000 grains (70% hcp Ti, 30% bcc beta-Ti, |g| <= 1.27,
+    15% noise peaks, cfg3 geometry) -> compute_xlylzl + compute_gv (FP64, fused
+    FP32 copy) -> batched scoring of n_ubi trial UBIs -> `rounds` rounds of
+    per-grain refinement (peaks grouped by their simulated grain) -> one
+    residual gradient over 12 geometry parameters + every UBI."""
+    from imaged11_b200 import adjoint, batch, synth
+    from imaged11_b200 import cImageD11 as cim
+    from imaged11_b200._lib import lib, check
+    truth = synth.default_geometry(**CFG3_TRUTH)
+    ng = 20000
+    rng = np.random.default_rng(SEED + 13)
+    cells = ["Ti_hcp" if x < 0.7 else "Ti_beta" for x in rng.random(ng)]
+    ps = synth.simulate(ng, gmax=1.27, seed=SEED + 13, geo=truth, noise_frac=0.15,
+                        translation=(5., -3., 2.), cells=cells)
+    n = len(ps)
+    trials = np.concatenate([
+        synth.trial_ubis(ps.ubis[np.array(cells) == c], int(n_ubi * frac), 0.1, 0.5, rng, cell=c)
+        for c, frac in (("Ti_hcp", 0.7), ("Ti_beta", 0.3))])
+    p, r, dist = synth.xlylzl_params(truth)
+    s_d = torch.tensor(ps.s, device=dev)
+    f_d = torch.tensor(ps.f, device=dev)
+    om_d = torch.tensor(ps.omega, device=dev)
+    xyz = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    gv = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    gs = batch.GvecSet(torch.zeros((n, 3), dtype=torch.float64, device=dev))
+    ub_d = torch.tensor(trials, device=dev)
+    idx, off = ps.grain_offsets()
+    idx_d = torch.tensor(idx, device=dev)
+    u_ref = synth.perturb_ubis(ps.ubis, 0.2, 0.002, rng)
+    stream = torch.cuda.current_stream().cuda_stream
+    t_arr = np.array([truth["t_x"], truth["t_y"], truth["t_z"]])
+    peaks = adjoint.PeakTable(ps.s[idx], ps.f[idx], ps.omega[idx], ps.hkl[idx], off, truth)
+    grains = batch.GrainSet(torch.zeros((len(idx), 3), dtype=torch.float64, device=dev), off,
+                            u_ref)
+    ws = batch.BatchWorkspace(len(trials), n, refine=False)
+
+    def run(ev):
+        ev[0].record()
+        cim.compute_xlylzl(s_d, f_d, p, r.ravel(), dist, xyz)
+        check(lib.id11b_dev_compute_gv(xyz.data_ptr(), om_d.data_ptr(), truth["omegasign"],
+                                       truth["wavelength"], truth["wedge"], truth["chi"],
+                                       t_arr.ctypes.data, gv.data_ptr(), gs.g4.data_ptr(), n,
+                                       stream), "compute_gv")
+        gs.gv = gv
+        gs.prepare()
+        ev[1].record()
+        c = batch.score_batch(ub_d, gs, [tol], workspace=ws)
+        ev[2].record()
+        torch.index_select(gv, 0, idx_d, out=grains.gv)
+        grains.ubis.copy_(torch.as_tensor(u_ref.reshape(-1, 9), device=dev))
+        grains.refine(tol, rounds)
+        ev[3].record()
+        pt = adjoint.params_tensor(truth).requires_grad_(True)
+        ut = grains.ubis.view(-1, 3, 3).clone().requires_grad_(True)
+        adjoint.loss(pt, ut, peaks).backward()
+        ev[4].record()
+        ev[4].synchronize()
+        return c
+
+    run([torch.cuda.Event(enable_timing=True) for _ in range(5)])   # warm-up (module loads)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    counts = run(ev)
+    names = ["compute_xlylzl+compute_gv", "score_batch", "refine_csr", "adjoint_gradient"]
+    stages = {}
+    for i, nm in enumerate(names):
+        stages[nm] = ev[i].elapsed_time(ev[i + 1])
+    pairs = n_ubi * n + rounds * grains.peaks + peaks.n
+    device_ms = sum(stages.values())
+    return {"grains": ng, "peaks": n, "trial_ubis": int(len(trials)), "tol": tol,
+            "stage_ms": stages, "pairs": pairs, "device_ms": device_ms,
+            "value": pairs / (device_ms * 1e-3), "unit": "pairs/s",
+            "trial_counts_median_max": [int(counts[:, 0].median().item()),
+                                        int(counts[:, 0].max().item())]}
+
+
 def workload(rank=0, n_ubi=N_UBI):
     from imaged11_b200 import synth
     ps = synth.simulate(N_GRAINS, "Al", gmax=GMAX, seed=SEED, noise_frac=0.10)
@@ -284,6 +407,12 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     ps, ubis = workload(rank, args.ubis)
+    if args.case == "adjoint":  # residual gradient (+ joint refinement)
+        print(json.dumps(adjoint_measure(torch, dev, steps=args.steps)))
+        return 0
+    if args.case == "pipeline":  # full-scale scan, end to end on the device
+        print(json.dumps(pipeline_measure(torch, dev)))
+        return 0
     if args.case == "refine":   # per-grain CSR refinement alone
         print(json.dumps(refine_csr_measure(torch, dev, steps=args.steps, cpu=False)))
         return 0
@@ -360,6 +489,7 @@ def run_ours(args, rank, world, local_rank):
     # uneven per-grain refinement (persistent kernel in a CUDA graph)
     refine = refine_csr_measure(torch, dev, steps=max(3, args.steps), flush=flush,
                                 cpu=(world == 1))
+    adj = adjoint_measure(torch, dev, steps=max(3, args.steps))
 
     # end to end through the public API: pinned host inputs -> counts on host
     gv_h = torch.tensor(ps.gv).pin_memory()
@@ -406,6 +536,7 @@ def run_ours(args, rank, world, local_rank):
                        "unit": "pairs/s", "ubis": m64,
                        "ratio_vs_per_tol": value / rate64, "ratio_vs_all_tols": value / rate64f},
         "refine_csr": refine,
+        "adjoint": adj,
         "compute_gv": {"peaks": 10_000_000, "ms": gv_ms, "achieved_gbs": gv_gbs,
                        "peak_gbs": hbm_peak, "peak_kind": hbm_kind,
                        "frac": gv_gbs / hbm_peak, "bytes_per_peak": 56},
@@ -428,7 +559,7 @@ def main():
     ap.add_argument("--ubis", type=int, default=N_UBI, help="trial UBIs per GPU")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed steps of the scoring step (profiling case)")
-    ap.add_argument("--case", default="score", choices=["score", "gv", "refine"],
+    ap.add_argument("--case", default="score", choices=["score", "gv", "refine", "adjoint", "pipeline"],
                     help="gv: compute_gv alone on --peaks lab positions; refine: per-grain "
                          "CSR refinement alone (profiling cases)")
     ap.add_argument("--peaks", type=int, default=10_000_000)

@@ -176,13 +176,17 @@ k_residual(AdjGeom P, const double* __restrict__ sc, const double* __restrict__ 
     }
 }
 
-// Sum rows of x (rows x cols) in row order -> out (cols); one CTA.
+// Column sums of x (rows x cols) -> out (cols); one CTA, one warp per column:
+// lane l sums rows l, l+32, ... in order, then a fixed butterfly, so the
+// result does not depend on timing.
 __global__ void k_sum_rows(const double* __restrict__ x, int rows, int cols,
                            double* __restrict__ out) {
-    for (int c = threadIdx.x; c < cols; c += blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    for (int c = threadIdx.x >> 5; c < cols; c += blockDim.x >> 5) {
         double t = 0.;
-        for (int r = 0; r < rows; r++) t += x[(int64_t)r * cols + c];
-        out[c] = t;
+        for (int r = lane; r < rows; r += 32) t += x[(int64_t)r * cols + c];
+        t = warp_sum(t);
+        if (lane == 0) out[c] = t;
     }
 }
 
@@ -244,7 +248,7 @@ extern "C" int id11b_dev_residuals_adjoint(const double* geom_host, const double
                                            nullptr, nullptr, nullptr, grad_res, grad_ubis,
                                            partial);
     ID11B_CHECK_LAUNCH();
-    k_sum_rows<<<1, 32, 0, st>>>(partial, ngrains, kGlob, grad_global);
+    k_sum_rows<<<1, 32 * kGlob, 0, st>>>(partial, ngrains, kGlob, grad_global);
     ID11B_CHECK_LAUNCH();
     return ID11B_OK;
 }

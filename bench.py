@@ -442,10 +442,13 @@ def run_ours(args, rank, world, local_rank):
     c64 = batch.score_many_fp64(ubis_d[:512], gs, TOLS)
     assert torch.equal(c64, counts[:512]), "FP32+recheck counts differ from FP64"
     if args.kernel_only:        # profiling case: warm-up + timed steps, nothing else
-        for _ in range(args.warmup + args.steps):
+        for _ in range(args.warmup):
             step()
+        kt = cuda_time_ms(torch, step, args.steps, flush)
         torch.cuda.synchronize()
-        print(json.dumps({"case": "score_batch", "ubis": m, "gvectors": n}))
+        print(json.dumps({"case": "score_batch", "ubis": m, "gvectors": n,
+                          "ms_per_step": sum(kt) / len(kt),
+                          "pairs_per_s": pairs / (sum(kt) / len(kt) * 1e-3)}))
         return 0
 
     for _ in range(args.warmup):

@@ -8,7 +8,9 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libimaged11_b200.so")
+# IMAGED11_B200_LIB may name another build of the same library (e.g. one
+# compiled with different tuning constants); default: the in-tree build.
+LIB_PATH = os.environ.get("IMAGED11_B200_LIB") or os.path.join(HERE, "libimaged11_b200.so")
 
 _d = ctypes.c_double
 _i = ctypes.c_int

@@ -23,9 +23,10 @@ def sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
-def build(verbose=False, extra=()):
-    """Compile every .cu under csrc/ and link libimaged11_b200.so."""
-    objdir = os.path.join(HERE, "_build")
+def build(verbose=False, extra=(), out=None, objdir=None):
+    """Compile every .cu under csrc/ and link libimaged11_b200.so (or `out`,
+    with extra nvcc flags such as -DID11B_SCORE_UBIS_PER_THREAD=8)."""
+    objdir = objdir or os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     objs = []
     for src in sources():
@@ -36,11 +37,11 @@ def build(verbose=False, extra=()):
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
+    cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", out or LIB, *objs]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
-    return LIB
+    return out or LIB
 
 
 if __name__ == "__main__":

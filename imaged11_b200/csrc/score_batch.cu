@@ -40,6 +40,12 @@
 namespace id11b {
 
 constexpr int kBT = 256;            // threads per CTA
+// UBIs held per thread by the screening kernel (even: screened in packed pairs)
+#ifndef ID11B_SCORE_UBIS_PER_THREAD
+#define ID11B_SCORE_UBIS_PER_THREAD 4
+#endif
+constexpr int kScoreR = ID11B_SCORE_UBIS_PER_THREAD;
+constexpr int kScoreCtasPerSm = kScoreR > 4 ? 2 : 3;
 constexpr int kTile = 1024;         // g per TMA tile (16 KB of float4)
 constexpr float kGLimit = 1024.f;   // larger |g_j| -> exact FP64 only
 constexpr double kEps32 = 5.9604644775390625e-08;  // 2^-24
@@ -233,7 +239,7 @@ __device__ __forceinline__ uint64_t drlv2_pair(const uint64_t up[9], uint64_t gx
 
 // ------------------------------------------------------------ main kernel --
 template <int R, int NT, int MODE>
-__global__ void __launch_bounds__(kBT, MODE == MODE_SCORE ? 3 : 2)
+__global__ void __launch_bounds__(kBT, MODE == MODE_SCORE ? kScoreCtasPerSm : 2)
 k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ g4,
         const double* __restrict__ gv, const double* __restrict__ ubis, int64_t n, int gsplit,
         Tols tols, const GvecInfo* __restrict__ gi, UbiInfo* __restrict__ ui,
@@ -537,11 +543,11 @@ struct UbiWs {  // layout of the per-call workspace
     size_t bytes;
 };
 
-static int ubis_per_cta(int mode) { return kBT * (mode == MODE_SCORE ? 4 : 2); }
+static int ubis_per_cta(int mode) { return kBT * (mode == MODE_SCORE ? kScoreR : 2); }
 
 static int choose_gsplit(int64_t m, int64_t n, int mode) {
     int64_t ublocks = (m + ubis_per_cta(mode) - 1) / ubis_per_cta(mode);
-    int64_t target = (int64_t)num_sms() * (mode == MODE_SCORE ? 3 : 2) * 4;  // ~4 waves
+    int64_t target = (int64_t)num_sms() * (mode == MODE_SCORE ? kScoreCtasPerSm : 2) * 4;  // ~4 waves
     int64_t gs = (target + ublocks - 1) / ublocks;
     int64_t maxgs = (n + kTile - 1) / kTile;  // at least one tile per CTA
     if (gs > maxgs) gs = maxgs;
@@ -573,7 +579,7 @@ static void launch_batch(int64_t m, int64_t n, int gsplit, const float4* packs, 
                          const double* gv, const double* ubis, const Tols& tols,
                          const GvecInfo* gi, UbiInfo* ui, int* counts, double* sums,
                          LsqAcc* part, cudaStream_t st) {
-    constexpr int R = MODE == MODE_SCORE ? 4 : 2;
+    constexpr int R = MODE == MODE_SCORE ? kScoreR : 2;
     const int64_t ublocks = (m + kBT * R - 1) / (kBT * R);
     size_t dyn = MODE == MODE_REFINE ? sizeof(double) * 17 * kBT * R
                                      : (sizeof(int) + sizeof(float)) * NT * kBT * R;

@@ -437,6 +437,11 @@ def run_ours(args, rank, world, local_rank):
         gs.prepare()
         batch.score_batch(ubis_d, gs, TOLS, workspace=ws, out=counts)
 
+    # launch shape from the autotuner (untimed setup; counts do not depend on it)
+    from imaged11_b200 import tune
+    gs.prepare()
+    tile, tune_table = tune.tune_score(ubis_d, gs, TOLS, reps=2)
+
     # correctness spot-check against the plain FP64 kernel (same assignments)
     step()
     c64 = batch.score_many_fp64(ubis_d[:512], gs, TOLS)
@@ -446,7 +451,7 @@ def run_ours(args, rank, world, local_rank):
             step()
         kt = cuda_time_ms(torch, step, args.steps, flush)
         torch.cuda.synchronize()
-        print(json.dumps({"case": "score_batch", "ubis": m, "gvectors": n,
+        print(json.dumps({"case": "score_batch", "ubis": m, "gvectors": n, "tile": tile,
                           "ms_per_step": sum(kt) / len(kt),
                           "pairs_per_s": pairs / (sum(kt) / len(kt) * 1e-3)}))
         return 0
@@ -526,13 +531,14 @@ def run_ours(args, rank, world, local_rank):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64recheck", "data": "synthetic",
-        "config": config_dict(n, m),
+        "config": dict(config_dict(n, m), tile={"ubis_per_thread": tile[0], "gsplit": tile[1]}),
+        "tuning_ms": {"%d,%d" % t: round(ms, 3) for t, ms in tune_table},
         "e2e": {"value": e2e_value, "unit": "pairs/s",
                 "h2d_bytes_per_step": int(ps.gv.nbytes + ubis.nbytes),
                 "d2h_bytes_per_step": int(m * T * 4)},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
-                     "kernel": "k_batch<4,3,score>",
+                     "kernel": "k_batch<%d,3,score>" % tile[0],
                      "peak_note": "CUDA-core FP32 = SMs x 128 x 2 x median SM clock under load; "
                                   "%d FLOP per (UBI,g) evaluation" % FLOP_PER_EVAL},
         "plain_fp64": {"value_per_tol_launch": rate64, "value_all_tols": rate64f,

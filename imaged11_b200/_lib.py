@@ -49,6 +49,9 @@ _SIGNATURES = [
     ("id11b_dev_prepare_gvecs", _i, [_p, _i64, _p, _p, _i64, _p]),
     ("id11b_batch_workspace_bytes", _i64, [_i64, _i64, _i]),
     ("id11b_dev_score_batch", _i, [_p, _i64, _p, _p, _i64, _p, _p, _i, _p, _p, _p, _i64, _p]),
+    ("id11b_score_tile_default", _i, [_i64, _i64, _p, _p]),
+    ("id11b_dev_score_batch_tiled", _i, [_p, _i64, _p, _p, _i64, _p, _p, _i, _p, _p, _i, _i,
+                                          _p, _i64, _p]),
     ("id11b_dev_refine_batch", _i, [_p, _i64, _p, _p, _i64, _p, _d, _i, _p, _p, _p, _i64, _p]),
     ("id11b_batch_stats", _i, [_p, _i64, _i64, _i, _p, _p, _p, _p]),
     ("id11b_refine_csr_workspace_bytes", _i64, []),

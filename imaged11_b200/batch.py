@@ -95,12 +95,14 @@ class BatchWorkspace:
         return nr.value, nf.value
 
 
-def score_batch(ubis, gvs, tols, sums=False, workspace=None, out=None):
+def score_batch(ubis, gvs, tols, sums=False, workspace=None, out=None, tile=None):
     """Counts of g-vectors indexed by each UBI at each tolerance.
 
     ubis: (m,3,3) float64 (numpy or CUDA); gvs: GvecSet; tols: 1-4 values.
     Returns an int32 CUDA tensor (m, len(tols)) -- and, with sums=True, the
-    float64 tensor of summed drlv2 of the counted pairs."""
+    float64 tensor of summed drlv2 of the counted pairs.
+    tile: (UBIs per thread, gsplit) launch shape; None takes the shape
+    tune.tune_score found for this size, else the built-in heuristic."""
     torch = _torch()
     u = _dev(ubis, torch.float64).reshape(-1, 9)
     m = u.shape[0]
@@ -110,10 +112,15 @@ def score_batch(ubis, gvs, tols, sums=False, workspace=None, out=None):
     counts = out if out is not None else torch.empty((m, len(t)), dtype=torch.int32,
                                                      device=u.device)
     s = torch.empty((m, len(t)), dtype=torch.float64, device=u.device) if sums else None
-    check(lib.id11b_dev_score_batch(u.data_ptr(), m, gvs.gv.data_ptr(), gvs.g4.data_ptr(),
-                                    gvs.n, gvs.ws.data_ptr(), t.ctypes.data, len(t),
-                                    counts.data_ptr(), s.data_ptr() if sums else None,
-                                    ws.buf.data_ptr(), ws.buf.numel(), _stream()),
+    if tile is None:
+        from . import tune
+        tile = tune.score_tile(m, gvs.n, len(t)) or (0, 0)
+    check(lib.id11b_dev_score_batch_tiled(u.data_ptr(), m, gvs.gv.data_ptr(),
+                                          gvs.g4.data_ptr(), gvs.n, gvs.ws.data_ptr(),
+                                          t.ctypes.data, len(t), counts.data_ptr(),
+                                          s.data_ptr() if sums else None, int(tile[0]),
+                                          int(tile[1]), ws.buf.data_ptr(), ws.buf.numel(),
+                                          _stream()),
           "score_batch")
     score_batch.last_workspace = ws
     return (counts, s) if sums else counts
@@ -168,12 +175,13 @@ class GrainSet:
     grain g owns gv[offsets[g]:offsets[g+1]]; ubis: (ngrains,3,3).  Everything
     is copied to the GPU once; grains are processed largest first.
 
-    threads: CTA size of the persistent launch.  Measured on B200 with 2,000
-    grains of 20..1,500 peaks: 64 threads 53 us for 5 rounds, 128 -> 87 us,
-    256 -> 147 us -- many small CTAs keep more grains in flight, which matters
-    more than the longest grain's share of lanes."""
+    threads: CTA size of the persistent launch; None takes the size
+    tune.tune_refine found for this many grains and peaks, else 64.  Measured
+    on B200 with 2,000 grains of 20..1,500 peaks: 64 threads 53 us for 5
+    rounds, 128 -> 87 us, 256 -> 147 us -- many small CTAs keep more grains in
+    flight, which matters more than the longest grain's share of lanes."""
 
-    def __init__(self, gv, offsets, ubis, threads=64):
+    def __init__(self, gv, offsets, ubis, threads=None):
         torch = _torch()
         self.gv = _dev(gv, torch.float64).reshape(-1, 3)
         off = np.ascontiguousarray(offsets, dtype=np.int64)
@@ -183,13 +191,16 @@ class GrainSet:
         sizes = np.diff(off)
         self.order = torch.as_tensor(np.argsort(-sizes, kind="stable").astype(np.int32),
                                      device=dev)
-        self.threads = int(threads)
         self.ubis = _dev(ubis, torch.float64).reshape(-1, 9).contiguous()
         self.npk = torch.zeros(self.ngrains, dtype=torch.int32, device=dev)
         self.mean = torch.zeros(self.ngrains, dtype=torch.float64, device=dev)
         self.ws = torch.zeros(lib.id11b_refine_csr_workspace_bytes(), dtype=torch.uint8,
                               device=dev)
         self.peaks = int(off[-1] - off[0]) if len(off) else 0
+        if threads is None:
+            from . import tune
+            threads = tune.refine_threads(self.ngrains, self.peaks) or 64
+        self.threads = int(threads)
 
     def refine(self, tol, iters, persistent=True):
         """Enqueue `iters` score_and_refine rounds for every grain (in place).

@@ -40,12 +40,14 @@
 namespace id11b {
 
 constexpr int kBT = 256;            // threads per CTA
-// UBIs held per thread by the screening kernel (even: screened in packed pairs)
+// UBIs held per thread by the screening kernel (even: screened in packed
+// pairs).  The default; id11b_dev_score_batch_tiled also offers 2.
 #ifndef ID11B_SCORE_UBIS_PER_THREAD
 #define ID11B_SCORE_UBIS_PER_THREAD 4
 #endif
 constexpr int kScoreR = ID11B_SCORE_UBIS_PER_THREAD;
-constexpr int kScoreCtasPerSm = kScoreR > 4 ? 2 : 3;
+// resident CTAs per SM the screening kernel is compiled for (register budget)
+__host__ __device__ constexpr int score_ctas_per_sm(int r) { return r <= 2 ? 4 : r <= 4 ? 3 : 2; }
 constexpr int kTile = 1024;         // g per TMA tile (16 KB of float4)
 constexpr float kGLimit = 1024.f;   // larger |g_j| -> exact FP64 only
 constexpr double kEps32 = 5.9604644775390625e-08;  // 2^-24
@@ -239,7 +241,7 @@ __device__ __forceinline__ uint64_t drlv2_pair(const uint64_t up[9], uint64_t gx
 
 // ------------------------------------------------------------ main kernel --
 template <int R, int NT, int MODE>
-__global__ void __launch_bounds__(kBT, MODE == MODE_SCORE ? kScoreCtasPerSm : 2)
+__global__ void __launch_bounds__(kBT, MODE == MODE_SCORE ? score_ctas_per_sm(R) : 2)
 k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ g4,
         const double* __restrict__ gv, const double* __restrict__ ubis, int64_t n, int gsplit,
         Tols tols, const GvecInfo* __restrict__ gi, UbiInfo* __restrict__ ui,
@@ -543,11 +545,14 @@ struct UbiWs {  // layout of the per-call workspace
     size_t bytes;
 };
 
-static int ubis_per_cta(int mode) { return kBT * (mode == MODE_SCORE ? kScoreR : 2); }
-
-static int choose_gsplit(int64_t m, int64_t n, int mode) {
-    int64_t ublocks = (m + ubis_per_cta(mode) - 1) / ubis_per_cta(mode);
-    int64_t target = (int64_t)num_sms() * (mode == MODE_SCORE ? kScoreCtasPerSm : 2) * 4;  // ~4 waves
+// g ranges per block of UBIs: about sixteen waves of CTAs (short CTAs balance
+// the tail; 20,000 UBIs x 1.1M g on B200: 17.8 ms vs 19.3 ms at four waves),
+// at least one g tile each
+static int choose_gsplit(int64_t m, int64_t n, int mode, int r) {
+    const int per_cta = kBT * r;
+    int64_t ublocks = (m + per_cta - 1) / per_cta;
+    int64_t target = (int64_t)num_sms() * (mode == MODE_SCORE ? score_ctas_per_sm(r) : 2) *
+                     (mode == MODE_SCORE ? 16 : 4);
     int64_t gs = (target + ublocks - 1) / ublocks;
     int64_t maxgs = (n + kTile - 1) / kTile;  // at least one tile per CTA
     if (gs > maxgs) gs = maxgs;
@@ -567,19 +572,19 @@ static UbiWs ubi_ws_layout(void* base, int64_t m, int64_t n, int mode) {
     off = align256(off + sizeof(float4) * 3 * (size_t)(m > 0 ? m : 1));
     w.part = (LsqAcc*)(b + off);
     if (mode == MODE_REFINE) {
-        int gs = choose_gsplit(m, n, mode);
+        int gs = choose_gsplit(m, n, mode, 2);
         off = align256(off + sizeof(LsqAcc) * (size_t)(gs + 1) * (size_t)(m > 0 ? m : 1));
     }
     w.bytes = off;
     return w;
 }
 
-template <int NT, int MODE>
+template <int R, int NT, int MODE>
 static void launch_batch(int64_t m, int64_t n, int gsplit, const float4* packs, const float4* g4,
                          const double* gv, const double* ubis, const Tols& tols,
                          const GvecInfo* gi, UbiInfo* ui, int* counts, double* sums,
                          LsqAcc* part, cudaStream_t st) {
-    constexpr int R = MODE == MODE_SCORE ? kScoreR : 2;
+    static_assert(MODE == MODE_SCORE || R == 2, "refinement keeps two UBIs per thread");
     const int64_t ublocks = (m + kBT * R - 1) / (kBT * R);
     size_t dyn = MODE == MODE_REFINE ? sizeof(double) * 17 * kBT * R
                                      : (sizeof(int) + sizeof(float)) * NT * kBT * R;
@@ -675,16 +680,38 @@ static int exact_lists(int mode, const double* ubis, int64_t m, const double* gv
     return ID11B_OK;
 }
 
-extern "C" int id11b_dev_score_batch(const double* ubis, int64_t m, const double* gv,
-                                     const float* g4, int64_t n, const void* gws,
-                                     const double* tols_host, int ntol, int32_t* counts,
-                                     double* sums, void* ws, int64_t ws_bytes, void* stream) {
+template <int R>
+static void launch_score(int ntol, int64_t m, int64_t n, int gsplit, const UbiWs& w,
+                         const float4* g4, const double* gv, const double* ubis, const Tols& T,
+                         const GvecInfo* gi, int* counts, double* sums, cudaStream_t st) {
+    switch (ntol) {
+        case 1: launch_batch<R, 1, MODE_SCORE>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
+        case 2: launch_batch<R, 2, MODE_SCORE>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
+        case 3: launch_batch<R, 3, MODE_SCORE>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
+        default: launch_batch<R, 4, MODE_SCORE>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
+    }
+}
+
+extern "C" int id11b_score_tile_default(int64_t m, int64_t n, int* ubis_per_thread, int* gsplit) {
+    if (m < 0 || n < 0 || !ubis_per_thread || !gsplit) return ID11B_ERR_ARG;
+    *ubis_per_thread = kScoreR;
+    *gsplit = choose_gsplit(m, n, MODE_SCORE, kScoreR);
+    return ID11B_OK;
+}
+
+extern "C" int id11b_dev_score_batch_tiled(const double* ubis, int64_t m, const double* gv,
+                                           const float* g4, int64_t n, const void* gws,
+                                           const double* tols_host, int ntol, int32_t* counts,
+                                           double* sums, int ubis_per_thread, int gsplit,
+                                           void* ws, int64_t ws_bytes, void* stream) {
     Tols T;
     int rc = check_tols(tols_host, ntol, T);
     if (rc) return rc;
     if (m < 0 || n < 0 || !ws || !gws || (m > 0 && (!ubis || !counts)) ||
         (n > 0 && (!gv || !g4)))
         return ID11B_ERR_ARG;
+    const int r = ubis_per_thread ? ubis_per_thread : kScoreR;
+    if ((r != 2 && r != 4 && r != kScoreR) || gsplit < 0) return ID11B_ERR_ARG;
     if (((uintptr_t)g4 & 15) || ((uintptr_t)ws & 255) || ((uintptr_t)gws & 255))
         return ID11B_ERR_ALIGN;
     if (ws_bytes < id11b_batch_workspace_bytes(m, n, 0)) return ID11B_ERR_SIZE;
@@ -700,15 +727,27 @@ extern "C" int id11b_dev_score_batch(const double* ubis, int64_t m, const double
     if (rc) return rc;
     if (m == 0 || n == 0) return ID11B_OK;
     const GvecInfo* gi = (const GvecInfo*)gws;
-    int gsplit = choose_gsplit(m, n, MODE_SCORE);
-    switch (ntol) {
-        case 1: launch_batch<1, MODE_SCORE>(m, n, gsplit, w.packs, (const float4*)g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
-        case 2: launch_batch<2, MODE_SCORE>(m, n, gsplit, w.packs, (const float4*)g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
-        case 3: launch_batch<3, MODE_SCORE>(m, n, gsplit, w.packs, (const float4*)g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
-        default: launch_batch<4, MODE_SCORE>(m, n, gsplit, w.packs, (const float4*)g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
-    }
+    const int64_t maxgs = (n + kTile - 1) / kTile;  // every CTA streams at least one tile
+    int gs = gsplit ? (int)(gsplit < maxgs ? gsplit : maxgs) : choose_gsplit(m, n, MODE_SCORE, r);
+    if (r == 2)
+        launch_score<2>(ntol, m, n, gs, w, (const float4*)g4, gv, ubis, T, gi, counts, sums, st);
+    else if (r == 4)
+        launch_score<4>(ntol, m, n, gs, w, (const float4*)g4, gv, ubis, T, gi, counts, sums, st);
+#if ID11B_SCORE_UBIS_PER_THREAD != 2 && ID11B_SCORE_UBIS_PER_THREAD != 4
+    else
+        launch_score<kScoreR>(ntol, m, n, gs, w, (const float4*)g4, gv, ubis, T, gi, counts,
+                              sums, st);
+#endif
     ID11B_CHECK_LAUNCH();
     return exact_lists(MODE_SCORE, ubis, m, gv, n, gws, w, T, ntol, counts, sums, nullptr, st);
+}
+
+extern "C" int id11b_dev_score_batch(const double* ubis, int64_t m, const double* gv,
+                                     const float* g4, int64_t n, const void* gws,
+                                     const double* tols_host, int ntol, int32_t* counts,
+                                     double* sums, void* ws, int64_t ws_bytes, void* stream) {
+    return id11b_dev_score_batch_tiled(ubis, m, gv, g4, n, gws, tols_host, ntol, counts, sums, 0,
+                                       0, ws, ws_bytes, stream);
 }
 
 extern "C" int id11b_dev_refine_batch(double* ubis, int64_t m, const double* gv, const float* g4,
@@ -728,7 +767,7 @@ extern "C" int id11b_dev_refine_batch(double* ubis, int64_t m, const double* gv,
     if (m == 0) return ID11B_OK;
     cudaStream_t st = (cudaStream_t)stream;
     UbiWs w = ubi_ws_layout(ws, m, n, MODE_REFINE);
-    const int gsplit = choose_gsplit(m, n, MODE_REFINE);
+    const int gsplit = choose_gsplit(m, n, MODE_REFINE, 2);
     const GvecInfo* gi = (const GvecInfo*)gws;
     for (int it = 0; it < iters; it++) {
         rc = prepare_ubis(ubis, m, gws, w, tol >= kTolLimit, st);
@@ -736,7 +775,7 @@ extern "C" int id11b_dev_refine_batch(double* ubis, int64_t m, const double* gv,
         // only the exact-list slot needs zeroing: every CTA writes its own slots
         ID11B_CHECK(cudaMemsetAsync(w.part + (int64_t)gsplit * m, 0, sizeof(LsqAcc) * m, st));
         if (n > 0) {
-            launch_batch<1, MODE_REFINE>(m, n, gsplit, w.packs, (const float4*)g4, gv, ubis, T,
+            launch_batch<2, 1, MODE_REFINE>(m, n, gsplit, w.packs, (const float4*)g4, gv, ubis, T,
                                          gi, w.info, nullptr, nullptr, w.part, st);
             ID11B_CHECK_LAUNCH();
             rc = exact_lists(MODE_REFINE, ubis, m, gv, n, gws, w, T, 1, nullptr, nullptr,

@@ -1,0 +1,171 @@
+"""Autotuner for the launch shapes of the batched kernels.
+
+The reference has no counterpart: it scores one UBI per call
+(ImageD11 src/closest.c:227-248) and refines one grain per call
+(src/closest.c:267-345).  Two shapes are tuned here, each by timing the
+candidates with CUDA events on the caller's own inputs:
+
+* score_batch tile -- UBIs per thread (2 or 4: 512 or 1,024 UBIs per CTA, held
+  in registers) x gsplit (how many g ranges each block of UBIs is split
+  into, i.e. how many 1,024-vector shared-memory tiles a CTA streams).
+  Counts are identical for every tile shape, so tuning needs no reference.
+* GrainSet CTA size for the persistent per-grain refinement (32..256).
+
+Results are cached per (device, shape bucket): m and n rounded up to powers of
+two.  ``save``/``load`` persist the cache as JSON; setting
+IMAGED11_B200_TUNE_CACHE to a file name loads it at import and makes
+``tune_score``/``tune_refine`` write it back.
+"""
+import json
+import math
+import os
+
+from ._lib import lib, check
+
+_cache = {}
+CACHE_ENV = "IMAGED11_B200_TUNE_CACHE"
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _bucket(x):
+    return 1 << max(0, int(math.ceil(math.log2(max(int(x), 1)))))
+
+
+def _device_name():
+    torch = _torch()
+    return torch.cuda.get_device_name(torch.cuda.current_device())
+
+
+def score_key(m, n, ntol):
+    return "score|%s|%d|%d|%d" % (_device_name(), _bucket(m), _bucket(n), int(ntol))
+
+
+def refine_key(ngrains, peaks):
+    return "refine|%s|%d|%d" % (_device_name(), _bucket(ngrains), _bucket(peaks))
+
+
+def default_score_tile(m, n):
+    """(UBIs per thread, gsplit) the built-in heuristic picks."""
+    import ctypes
+    r = ctypes.c_int(0)
+    g = ctypes.c_int(0)
+    check(lib.id11b_score_tile_default(int(m), int(n), ctypes.addressof(r), ctypes.addressof(g)),
+          "score_tile_default")
+    return r.value, g.value
+
+
+def score_candidates(m, n):
+    """Tile shapes tried by tune_score: both register blockings, each with the
+    heuristic's g split scaled by 1/8 .. 4 (at most one tile per CTA)."""
+    maxgs = max(1, -(-int(n) // 1024))
+    out = []
+    for r in (4, 2):
+        per = 256 * r
+        ublocks = max(1, -(-int(m) // per))
+        # the heuristic's split for this blocking: ~16 waves of resident CTAs
+        torch = _torch()
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        base = max(1, -(-(sms * (3 if r == 4 else 4) * 16) // ublocks))
+        for f in (0.125, 0.25, 0.5, 1.0, 2.0, 4.0):
+            gs = int(min(maxgs, max(1, round(base * f))))
+            if (r, gs) not in out:
+                out.append((r, gs))
+    return out
+
+
+def _time(fn, reps):
+    torch = _torch()
+    st = torch.cuda.current_stream()
+    fn()  # warm-up (also loads the kernel)
+    best = float("inf")
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
+def tune_score(ubis, gvs, tols, reps=3, candidates=None):
+    """Time every candidate tile shape of score_batch on these inputs, cache
+    the fastest for this shape bucket and return (tile, [(tile, ms), ...])."""
+    from . import batch
+    torch = _torch()
+    u = batch._dev(ubis, torch.float64).reshape(-1, 9)
+    m = u.shape[0]
+    ws = batch.BatchWorkspace(m, gvs.n, False)
+    out = torch.empty((m, len(batch._tols(tols))), dtype=torch.int32, device=u.device)
+    table = []
+    for tile in candidates or score_candidates(m, gvs.n):
+        ms = _time(lambda: batch.score_batch(u, gvs, tols, workspace=ws, out=out, tile=tile),
+                   reps)
+        table.append((tuple(tile), ms))
+    best = min(table, key=lambda x: x[1])[0]
+    _cache[score_key(m, gvs.n, len(batch._tols(tols)))] = list(best)
+    _autosave()
+    return best, table
+
+
+def score_tile(m, n, ntol):
+    """The tuned tile for this shape bucket, or None (use the heuristic)."""
+    if not _cache:
+        return None
+    t = _cache.get(score_key(m, n, ntol))
+    return tuple(t) if t else None
+
+
+def tune_refine(grains, tol, iters, reps=3, threads=(32, 64, 128, 256)):
+    """Time the persistent refinement of a GrainSet at each CTA size (UBIs are
+    restored after every trial), set grains.threads to the fastest, cache it
+    and return (threads, [(threads, ms), ...])."""
+    saved = grains.ubis.clone()
+    table = []
+    for t in threads:
+        def run():
+            grains.ubis.copy_(saved)
+            grains._launch(tol, iters, 1, t)
+        table.append((t, _time(run, reps)))
+    grains.ubis.copy_(saved)
+    best = min(table, key=lambda x: x[1])[0]
+    grains.threads = best
+    _cache[refine_key(grains.ngrains, grains.peaks)] = best
+    _autosave()
+    return best, table
+
+
+def refine_threads(ngrains, peaks):
+    """The tuned CTA size for this shape bucket, or None."""
+    if not _cache:
+        return None
+    return _cache.get(refine_key(ngrains, peaks))
+
+
+def save(path):
+    with open(path, "w") as f:
+        json.dump(_cache, f, indent=1, sort_keys=True)
+
+
+def load(path):
+    with open(path) as f:
+        _cache.update(json.load(f))
+
+
+def clear():
+    _cache.clear()
+
+
+def _autosave():
+    p = os.environ.get(CACHE_ENV)
+    if p:
+        save(p)
+
+
+if os.environ.get(CACHE_ENV) and os.path.exists(os.environ[CACHE_ENV]):
+    load(os.environ[CACHE_ENV])

@@ -202,6 +202,20 @@ int id11b_dev_score_batch(const double *ubis, int64_t m, const double *gv, const
                           int32_t *counts, double *sums, void *ws, int64_t ws_bytes,
                           void *stream);
 
+/* id11b_dev_score_batch with an explicit tile shape (no reference counterpart:
+ * the reference scores one UBI per call).  A CTA holds 256 * ubis_per_thread
+ * UBIs in registers (2 or 4; 0 = the build default, 4) and streams 1/gsplit of
+ * the g-vectors through shared memory in 1,024-vector tiles (gsplit 0 = the
+ * built-in heuristic, about four waves of CTAs; larger values are clamped to
+ * one tile per CTA).  Counts do not depend on the tile shape.
+ * id11b_score_tile_default reports the shape the heuristic picks. */
+int id11b_score_tile_default(int64_t m, int64_t n, int *ubis_per_thread, int *gsplit);
+int id11b_dev_score_batch_tiled(const double *ubis, int64_t m, const double *gv,
+                                const float *g4, int64_t n, const void *gws,
+                                const double *tols_host, int ntol, int32_t *counts,
+                                double *sums, int ubis_per_thread, int gsplit, void *ws,
+                                int64_t ws_bytes, void *stream);
+
 /* `iters` rounds of score_and_refine (ImageD11 src/closest.c:267-345) for each
  * of m UBIs against all n g-vectors, ubis (m,3,3) updated in place; npk and
  * mean_drlv2 (optional) receive the last round's count and mean drlv2.

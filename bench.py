@@ -68,6 +68,41 @@ def compute_gv_measure(torch, ps, dev, n_peaks=10_000_000, steps=5, flush=None):
     return 56.0 * n_peaks / (ms * 1e-3) / 1e9, ms
 
 
+def grid_measure(torch, dev, ps, ubis, steps=5, flush=None, check_counts=None, cell=None):
+    """Scoring through the reciprocal-space cell index on the same workload:
+    index build time, ms per score_grid call (inputs resident, L2 flushed
+    between calls) and pairs decided per second."""
+    from imaged11_b200 import batch
+    gv_d = torch.tensor(ps.gv, device=dev)
+    ubis_d = torch.tensor(ubis, device=dev)
+    m, n, T = len(ubis), len(ps.gv), len(TOLS)
+    batch.GvecGrid(gv_d, cell=cell)                       # load the kernels
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    grid = batch.GvecGrid(gv_d, cell=cell)
+    torch.cuda.synchronize()
+    build_ms = (time.perf_counter() - t0) * 1e3
+    ws = torch.empty(batch.lib.id11b_grid_score_workspace_bytes(m, T), dtype=torch.uint8,
+                     device=dev)
+    counts = torch.empty((m, T), dtype=torch.int32, device=dev)
+
+    def run():
+        batch.score_grid(ubis_d, grid, TOLS, workspace=ws, out=counts)
+    for _ in range(3):
+        run()
+    same = None
+    if check_counts is not None:
+        same = bool(torch.equal(counts, check_counts))
+    times = cuda_time_ms(torch, run, steps, flush)
+    ms = float(np.mean(times))
+    st = grid.stats()
+    return {"ms": ms, "value": m * n * T / (ms * 1e-3), "unit": "pairs/s",
+            "build_ms_wall": build_ms, "cells": grid.nx ** 3, "cell_A^-1": grid.cs,
+            "pairs_tested_fp64": st["pairs_tested"],
+            "tested_fraction": st["pairs_tested"] / float(m * n),
+            "plain_scan_ubis": st["fallback_ubis"], "counts_equal_score_batch": same}
+
+
 def refine_workload(seed=SEED + 7, ngrains=2000):
     """Uneven per-grain refinement: hcp Ti grains (a=2.95, c=4.68 A), per-grain
     peak counts log-uniform in 20..2000 set by a per-grain |g| cutoff (capped by
@@ -416,6 +451,10 @@ def run_ours(args, rank, world, local_rank):
     if args.case == "refine":   # per-grain CSR refinement alone
         print(json.dumps(refine_csr_measure(torch, dev, steps=args.steps, cpu=False)))
         return 0
+    if args.case == "grid":     # cell-index scoring alone (profiling case)
+        for cell in (args.cell or [None]):
+            print(json.dumps(grid_measure(torch, dev, ps, ubis, steps=args.steps, cell=cell)))
+        return 0
     if args.case == "gv":       # compute_gv alone (profiling case)
         gbs, ms = compute_gv_measure(torch, ps, dev, args.peaks, args.steps)
         print(json.dumps({"case": "compute_gv", "peaks": args.peaks, "GB/s": gbs, "ms": ms}))
@@ -568,10 +607,12 @@ def main():
     ap.add_argument("--ubis", type=int, default=N_UBI, help="trial UBIs per GPU")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed steps of the scoring step (profiling case)")
-    ap.add_argument("--case", default="score", choices=["score", "gv", "refine", "adjoint", "pipeline"],
+    ap.add_argument("--case", default="score",
+                    choices=["score", "gv", "grid", "refine", "adjoint", "pipeline"],
                     help="gv: compute_gv alone on --peaks lab positions; refine: per-grain "
                          "CSR refinement alone (profiling cases)")
     ap.add_argument("--peaks", type=int, default=10_000_000)
+    ap.add_argument("--cell", type=float, nargs="*", help="grid case: cell sides (1/A) to time")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

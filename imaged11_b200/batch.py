@@ -126,6 +126,69 @@ def score_batch(ubis, gvs, tols, sums=False, workspace=None, out=None, tile=None
     return (counts, s) if sums else counts
 
 
+class GvecGrid:
+    """Reciprocal-space cell index of a set of g-vectors, for score_grid.
+
+    gv: (n,3) float64 (numpy or CUDA) or a GvecSet.  cell: side of the cubic
+    cells in 1/Angstrom (None: about one g per cell of the bounding cube).
+    Building reads two numbers back to the host (the bounds that size the
+    grid); scoring does not."""
+
+    def __init__(self, gv, cell=None):
+        import ctypes
+        torch = _torch()
+        g = gv.gv if isinstance(gv, GvecSet) else _dev(gv, torch.float64).reshape(-1, 3)
+        self.gv = g.contiguous()
+        self.n = self.gv.shape[0]
+        dev = self.gv.device
+        bounds = torch.zeros(2, dtype=torch.int32, device=dev)
+        check(lib.id11b_dev_gvec_bounds(self.gv.data_ptr(), self.n, bounds.data_ptr(),
+                                        _stream()), "gvec_bounds")
+        b = bounds.cpu().numpy().view(np.float32)
+        self.gmax, self.rmax = float(b[0]), float(b[1])
+        nx = ctypes.c_int32(0)
+        cs = ctypes.c_double(0.)
+        check(lib.id11b_grid_plan(self.gmax, self.n, float(cell or 0.), ctypes.addressof(nx),
+                                  ctypes.addressof(cs)), "grid_plan")
+        self.nx, self.cs = nx.value, cs.value
+        nbytes = lib.id11b_grid_bytes(self.n, self.nx)
+        self.buf = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        check(lib.id11b_dev_build_grid(self.gv.data_ptr(), self.n, self.gmax, self.rmax,
+                                       self.cs, self.nx, self.buf.data_ptr(), nbytes,
+                                       _stream()), "build_grid")
+
+    def stats(self):
+        """dict: regular / listed g-vectors; UBIs scanned plainly and pairs
+        evaluated by the last score_grid call (synchronises)."""
+        import ctypes
+        v = [ctypes.c_int64(0) for _ in range(4)]
+        check(lib.id11b_grid_stats(self.buf.data_ptr(), *[ctypes.addressof(x) for x in v],
+                                   _stream()), "grid_stats")
+        return dict(zip(("regular", "special", "fallback_ubis", "pairs_tested"),
+                        (x.value for x in v)))
+
+
+def score_grid(ubis, grid, tols, sums=False, workspace=None, out=None):
+    """score_batch through the cell index: the same counts (and, with
+    sums=True, FP64 sums of the counted drlv2) for every UBI and tolerance,
+    testing only the g-vectors near each UB.hkl.  grid: GvecGrid."""
+    torch = _torch()
+    u = _dev(ubis, torch.float64).reshape(-1, 9)
+    m = u.shape[0]
+    t = _tols(tols)
+    need = lib.id11b_grid_score_workspace_bytes(m, len(t))
+    ws = workspace if workspace is not None and workspace.numel() >= need else \
+        torch.empty(need, dtype=torch.uint8, device=u.device)
+    counts = out if out is not None else torch.empty((m, len(t)), dtype=torch.int32,
+                                                     device=u.device)
+    s = torch.empty((m, len(t)), dtype=torch.float64, device=u.device) if sums else None
+    check(lib.id11b_dev_score_grid(u.data_ptr(), m, grid.gv.data_ptr(), grid.n, grid.nx,
+                                   grid.buf.data_ptr(), t.ctypes.data, len(t), counts.data_ptr(),
+                                   s.data_ptr() if sums else None, ws.data_ptr(), ws.numel(),
+                                   _stream()), "score_grid")
+    return (counts, s) if sums else counts
+
+
 def score_many_fp64(ubis, gv, tols, out=None):
     """Plain FP64 batched score (reference arithmetic).  gv: (n,3) float64 CUDA
     tensor or GvecSet.  Returns int32 (m, len(tols))."""

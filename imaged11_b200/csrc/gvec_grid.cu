@@ -1,0 +1,944 @@
+// Reciprocal-space cell index over the g-vectors, and scoring by hkl lookup.
+//
+// The reference's score() (ImageD11 src/closest.c:227-248) tests every g
+// against a UBI.  A g-vector is counted iff |UBI.g - round(UBI.g)|^2 < tol^2,
+// i.e. iff it lies inside the ellipsoid of radius tol (in hkl units) around
+// UB.hkl for hkl = round(UBI.g), UB = UBI^-1.  This file bins the g-vectors
+// into a uniform grid of cubic cells (x fastest, so a row of cells along x is
+// one contiguous range of the cell-sorted g), then for each UBI enumerates
+// the integer hkl whose ellipsoid can reach the data and tests only the g in
+// the cells overlapping a conservative bounding box of that ellipsoid.  Every
+// tested pair is evaluated with the reference's exact FP64 arithmetic
+// (drlv2_exact) and counted only under its own hkl (ih == hkl), so each g is
+// counted at most once and exactly when the reference counts it.
+//
+// Conservativeness: with d = UBI.g - hkl, g = UB.hkl + UB.d, so
+// |g_j - (UB.hkl)_j| <= |d| * ||row j of UB||.  The box half-widths use
+// (tol + 1e-6) in place of |d|: 1e-6 in hkl units is far above the FP64
+// rounding of h, of UB = inv(UBI) (condition number capped at 1e6) and of
+// UB.hkl (|hkl| capped).  Cell coordinates come from one monotone function
+// of a coordinate, used by the build and the query alike, so a g inside the
+// box is always inside the scanned cells.  UBIs outside the caps (non-finite,
+// singular, ill-conditioned, or with more candidate hkl than g-vectors) are
+// scored by a plain scan of every regular g; g-vectors outside the regular
+// range (non-finite or |g_j| > 1024) by a scan over that list.
+#include <math.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace id11b {
+namespace grid {
+
+constexpr int kGT = 256;           // threads per CTA (8 warps, one warp per work item)
+constexpr int kScanT = 1024;       // scan CTA
+constexpr int kScanPer = 4 * kScanT;
+constexpr double kGLimit = 1024.0;  // regular g: finite, every |g_j| <= 1024
+constexpr double kHklMargin = 1e-6;
+constexpr double kMaxCond = 1e6;
+constexpr int kMaxParts = 64;
+
+struct Header {
+    double lo, cs, inv_cs;  // cube [lo, lo + nx*cs)^3
+    double rmax;            // max |g| over regular g (rounded up)
+    int64_t ncells;
+    int64_t n;
+    int32_t nx;
+    int32_t pad;
+    unsigned long long nfallback;  // UBIs scored by the plain scan (last call)
+    unsigned long long ntested;    // (UBI, g) pairs evaluated in FP64 (last call)
+};
+
+struct Tols {
+    double t[ID11B_MAX_TOLS];
+};
+
+__host__ __device__ inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Grid buffer: header | cnt[ncells+1] | start[ncells+1] | g[n][3] | g4[n] | gidx[n] |
+// flag[n+1] | spos[n+1] | spec[n] | scan totals
+struct Layout {
+    size_t header, cnt, start, g, g4, idx, flag, spos, spec, tot, bytes;
+};
+
+__host__ __device__ inline Layout layout(int64_t n, int64_t ncells) {
+    Layout L;
+    const size_t nn = (size_t)(n > 0 ? n : 1);
+    const int64_t big = ncells + 1 > n + 1 ? ncells + 1 : n + 1;
+    size_t o = 0;
+    L.header = o; o = al256(o + sizeof(Header));
+    L.cnt = o;    o = al256(o + sizeof(int) * (size_t)(ncells + 1));
+    L.start = o;  o = al256(o + sizeof(int) * (size_t)(ncells + 1));
+    L.g = o;      o = al256(o + sizeof(double) * 3 * nn);
+    L.g4 = o;     o = al256(o + sizeof(float4) * nn);
+    L.idx = o;    o = al256(o + sizeof(int) * nn);
+    L.flag = o;   o = al256(o + sizeof(int) * (nn + 1));
+    L.spos = o;   o = al256(o + sizeof(int) * (nn + 1));
+    L.spec = o;   o = al256(o + sizeof(int) * nn);
+    L.tot = o;    o = al256(o + sizeof(int) * (size_t)((big + kScanPer - 1) / kScanPer + 1));
+    L.bytes = o;
+    return L;
+}
+
+__device__ __forceinline__ bool regular(double a, double b, double c) {
+    double m = fmax(fabs(a), fmax(fabs(b), fabs(c)));
+    return isfinite(a) && isfinite(b) && isfinite(c) && m <= kGLimit;
+}
+
+// Monotone in x (RN subtraction and multiplication by a positive constant,
+// clamp, truncation of a non-negative value); NaN must not reach it.
+__device__ __forceinline__ int coord(double x, const Header& H) {
+    double f = __dmul_rn(__dsub_rn(x, H.lo), H.inv_cs);
+    f = fmin(fmax(f, 0.0), (double)(H.nx - 1));
+    return (int)f;
+}
+
+__device__ __forceinline__ int64_t cell_of(double a, double b, double c, const Header& H) {
+    return ((int64_t)coord(c, H) * H.nx + coord(b, H)) * H.nx + coord(a, H);
+}
+
+// ------------------------------------------------------------------ build --
+// max |g_j| and max |g| over regular g, as float bits rounded up
+__global__ void __launch_bounds__(kGT)
+k_bounds(const double* __restrict__ gv, int64_t n, unsigned int* __restrict__ out) {
+    float gm = 0.f, rm = 0.f;
+    for (int64_t k = (int64_t)blockIdx.x * kGT + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * kGT) {
+        double a = gv[3 * k], b = gv[3 * k + 1], c = gv[3 * k + 2];
+        if (!regular(a, b, c)) continue;
+        gm = fmaxf(gm, __double2float_ru(fmax(fabs(a), fmax(fabs(b), fabs(c)))));
+        rm = fmaxf(rm, __double2float_ru(sqrt(a * a + b * b + c * c) * (1. + 1e-12)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        gm = fmaxf(gm, __shfl_xor_sync(0xffffffffu, gm, o));
+        rm = fmaxf(rm, __shfl_xor_sync(0xffffffffu, rm, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out, __float_as_uint(gm));
+        atomicMax(out + 1, __float_as_uint(rm));
+    }
+}
+
+__global__ void __launch_bounds__(kGT)
+k_count(const double* __restrict__ gv, int64_t n, const Header* __restrict__ Hp,
+        int* __restrict__ cnt, int* __restrict__ flag) {
+    const Header H = *Hp;
+    for (int64_t k = (int64_t)blockIdx.x * kGT + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * kGT) {
+        double a = gv[3 * k], b = gv[3 * k + 1], c = gv[3 * k + 2];
+        const bool reg = regular(a, b, c);
+        flag[k] = reg ? 0 : 1;
+        if (reg) atomicAdd(cnt + cell_of(a, b, c, H), 1);
+    }
+}
+
+// exclusive scan of x[0..len) into y, CTA totals into tot (pass 1)
+__global__ void __launch_bounds__(kScanT)
+k_scan_local(const int* __restrict__ x, int64_t len, int* __restrict__ y, int* __restrict__ tot) {
+    __shared__ int s_w[kScanT / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanPer + 4 * threadIdx.x;
+    int v[4], sum = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        v[q] = base + q < len ? x[base + q] : 0;
+        sum += v[q];
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_w[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int w = s_w[lane];
+        int wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        s_w[lane] = wi - w;  // exclusive over warps
+        if (lane == 31) tot[blockIdx.x] = wi;
+    }
+    __syncthreads();
+    int run = s_w[wid] + incl - sum;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (base + q < len) y[base + q] = run;
+        run += v[q];
+    }
+}
+
+// exclusive scan of the CTA totals in place (one CTA, sequential chunks)
+__global__ void __launch_bounds__(kScanT) k_scan_totals(int* __restrict__ tot, int nb) {
+    __shared__ int s_w[kScanT / 32];
+    __shared__ int s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int b0 = 0; b0 < nb; b0 += kScanT) {
+        const int i = b0 + threadIdx.x;
+        const int v = i < nb ? tot[i] : 0;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) s_w[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            int w = s_w[lane], wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int t = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += t;
+            }
+            s_w[lane] = wi - w;
+        }
+        __syncthreads();
+        const int carry = s_carry;
+        if (i < nb) tot[i] = carry + s_w[wid] + incl - v;
+        __syncthreads();
+        if (threadIdx.x == kScanT - 1) s_carry = carry + s_w[wid] + incl;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kScanT)
+k_scan_add(int* __restrict__ y, int64_t len, const int* __restrict__ tot) {
+    const int64_t base = (int64_t)blockIdx.x * kScanPer + 4 * threadIdx.x;
+    const int add = tot[blockIdx.x];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+        if (base + q < len) y[base + q] += add;
+}
+
+__global__ void __launch_bounds__(kGT)
+k_scatter(const double* __restrict__ gv, int64_t n, const Header* __restrict__ Hp,
+          const int* __restrict__ start, int* __restrict__ cursor, double* __restrict__ gs,
+          int* __restrict__ gidx, const int* __restrict__ spos, int* __restrict__ spec) {
+    const Header H = *Hp;
+    for (int64_t k = (int64_t)blockIdx.x * kGT + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * kGT) {
+        double a = gv[3 * k], b = gv[3 * k + 1], c = gv[3 * k + 2];
+        if (!regular(a, b, c)) {
+            spec[spos[k]] = (int)k;
+            continue;
+        }
+        const int64_t cid = cell_of(a, b, c, H);
+        const int p = start[cid] + atomicAdd(cursor + cid, 1);
+        gs[3 * (int64_t)p] = a;
+        gs[3 * (int64_t)p + 1] = b;
+        gs[3 * (int64_t)p + 2] = c;
+        gidx[p] = (int)k;
+    }
+}
+
+// order each cell's entries by original index: the layout, and so every
+// result, does not depend on the order the scatter's atomics ran in
+__global__ void __launch_bounds__(kGT)
+k_sort_cells(const int* __restrict__ start, int64_t ncells, double* __restrict__ gs,
+             int* __restrict__ gidx, float4* __restrict__ g4) {
+    for (int64_t c = (int64_t)blockIdx.x * kGT + threadIdx.x; c < ncells;
+         c += (int64_t)gridDim.x * kGT) {
+        const int a = start[c], b = start[c + 1];
+        for (int i = a + 1; i < b; i++) {
+            const int key = gidx[i];
+            const double x = gs[3 * (int64_t)i], y = gs[3 * (int64_t)i + 1],
+                         z = gs[3 * (int64_t)i + 2];
+            int j = i - 1;
+            while (j >= a && gidx[j] > key) {
+                gidx[j + 1] = gidx[j];
+                gs[3 * (int64_t)j + 3] = gs[3 * (int64_t)j];
+                gs[3 * (int64_t)j + 4] = gs[3 * (int64_t)j + 1];
+                gs[3 * (int64_t)j + 5] = gs[3 * (int64_t)j + 2];
+                j--;
+            }
+            gidx[j + 1] = key;
+            gs[3 * (int64_t)j + 3] = x;
+            gs[3 * (int64_t)j + 4] = y;
+            gs[3 * (int64_t)j + 5] = z;
+        }
+        for (int i = a; i < b; i++)
+            g4[i] = make_float4((float)gs[3 * (int64_t)i], (float)gs[3 * (int64_t)i + 1],
+                                (float)gs[3 * (int64_t)i + 2], 0.f);
+    }
+}
+
+// ------------------------------------------------------------- per UBI ----
+// Query plan of one UBI (uniform across the warp).
+struct Plan {
+    double ub[9];      // UBI^-1
+    double w[3];       // box half-widths
+    int64_t lo[3];     // hkl box
+    int64_t nh[3];
+    int64_t total;     // hkl in the box
+    bool ok;           // false: plain scan of every regular g
+};
+
+__device__ __forceinline__ Plan make_plan(const double u[9], double tmax, const Header& H,
+                                          int64_t nreg) {
+    Plan P;
+    bool ok = true;
+#pragma unroll
+    for (int e = 0; e < 9; e++) ok = ok && isfinite(u[e]);
+    const double c00 = u[4] * u[8] - u[5] * u[7], c01 = u[5] * u[6] - u[3] * u[8],
+                 c02 = u[3] * u[7] - u[4] * u[6];
+    const double det = u[0] * c00 + u[1] * c01 + u[2] * c02;
+    ok = ok && isfinite(det) && det != 0.;
+    const double id = 1.0 / det;
+    P.ub[0] = c00 * id;
+    P.ub[1] = (u[2] * u[7] - u[1] * u[8]) * id;
+    P.ub[2] = (u[1] * u[5] - u[2] * u[4]) * id;
+    P.ub[3] = c01 * id;
+    P.ub[4] = (u[0] * u[8] - u[2] * u[6]) * id;
+    P.ub[5] = (u[2] * u[3] - u[0] * u[5]) * id;
+    P.ub[6] = c02 * id;
+    P.ub[7] = (u[1] * u[6] - u[0] * u[7]) * id;
+    P.ub[8] = (u[0] * u[4] - u[1] * u[3]) * id;
+    double nu = 0., nb = 0.;
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+        nu += u[e] * u[e];
+        nb += P.ub[e] * P.ub[e];
+        ok = ok && isfinite(P.ub[e]);
+    }
+    ok = ok && sqrt(nu) * sqrt(nb) <= kMaxCond;
+    const double G = -H.lo;  // every regular g lies in [-G, G]^3
+    double total = 1.;
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const double s = fabs(u[3 * r]) + fabs(u[3 * r + 1]) + fabs(u[3 * r + 2]);
+        const double hm = s * G + 1.0;
+        ok = ok && hm < 1e6;
+        const double l = floor(-hm), h = ceil(hm);
+        P.lo[r] = ok ? (int64_t)l : 0;
+        P.nh[r] = ok ? (int64_t)(h - l) + 1 : 1;
+        total *= (h - l) + 1.;
+        P.w[r] = (tmax + kHklMargin) *
+                 sqrt(P.ub[3 * r] * P.ub[3 * r] + P.ub[3 * r + 1] * P.ub[3 * r + 1] +
+                      P.ub[3 * r + 2] * P.ub[3 * r + 2]) * (1. + 1e-9);
+        ok = ok && isfinite(P.w[r]);
+    }
+    ok = ok && total <= (double)nreg;  // more candidate hkl than g: the plain scan is cheaper
+    P.total = ok ? P.nh[0] * P.nh[1] * P.nh[2] : 0;
+    P.ok = ok;
+    return P;
+}
+
+__device__ __forceinline__ void hkl_of(const Plan& P, int64_t q, double hkl[3]) {
+    const int64_t i0 = q % P.nh[0], rest = q / P.nh[0];
+    const int64_t i1 = rest % P.nh[1], i2 = rest / P.nh[1];
+    hkl[0] = (double)(P.lo[0] + i0);
+    hkl[1] = (double)(P.lo[1] + i1);
+    hkl[2] = (double)(P.lo[2] + i2);
+}
+
+__device__ __forceinline__ void centre(const Plan& P, const double hkl[3], double c[3]) {
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+        c[r] = P.ub[3 * r] * hkl[0] + P.ub[3 * r + 1] * hkl[1] + P.ub[3 * r + 2] * hkl[2];
+}
+
+// can the box around c reach a regular g?
+__device__ __forceinline__ bool reaches(const Plan& P, const double c[3], const Header& H) {
+    const double G = -H.lo;
+    bool in = true;
+    double d2 = 0.;
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        in = in && (c[r] - P.w[r] <= G) && (c[r] + P.w[r] >= -G);
+        // distance from the origin to the nearest point of the box, per axis
+        const double e = fmax(fabs(c[r]) - P.w[r], 0.);
+        d2 += e * e;
+    }
+    return in && d2 <= H.rmax * H.rmax * (1. + 1e-9);
+}
+
+// Visit the g inside the box around c (one lane, one hkl): fn(pos, g0, g1, g2).
+// Rows of cells along x are contiguous ranges of the cell-sorted g.  The FP32
+// copy filters first with half-widths w32 widened past every FP32 rounding
+// (so it never rejects a g of the FP64 box); the FP64 box test follows.
+template <class Fn>
+__device__ __forceinline__ void visit_box(const double c[3], const double w[3],
+                                          const float w32[3], const Header& H,
+                                          const int* __restrict__ start,
+                                          const double* __restrict__ gs,
+                                          const float4* __restrict__ g4, Fn&& fn) {
+    const int ix0 = coord(c[0] - w[0], H), ix1 = coord(c[0] + w[0], H);
+    const int iy0 = coord(c[1] - w[1], H), iy1 = coord(c[1] + w[1], H);
+    const int iz0 = coord(c[2] - w[2], H), iz1 = coord(c[2] + w[2], H);
+    const float cx = (float)c[0], cy = (float)c[1], cz = (float)c[2];
+    for (int iz = iz0; iz <= iz1; iz++)
+        for (int iy = iy0; iy <= iy1; iy++) {
+            const int64_t row = ((int64_t)iz * H.nx + iy) * H.nx;
+            const int st = __ldg(start + row + ix0), en = __ldg(start + row + ix1 + 1);
+            for (int p = st; p < en; p++) {
+                const float4 v = __ldg(g4 + p);
+                if (fabsf(v.x - cx) <= w32[0] && fabsf(v.y - cy) <= w32[1] &&
+                    fabsf(v.z - cz) <= w32[2]) {
+                    const double g0 = __ldg(gs + 3 * (int64_t)p),
+                                 g1 = __ldg(gs + 3 * (int64_t)p + 1),
+                                 g2 = __ldg(gs + 3 * (int64_t)p + 2);
+                    if (fabs(g0 - c[0]) <= w[0] && fabs(g1 - c[1]) <= w[1] &&
+                        fabs(g2 - c[2]) <= w[2])
+                        fn(p, g0, g1, g2);
+                }
+            }
+        }
+}
+
+// Per-warp queue of hkl that reach the data.  Enumeration: 32 (h, k) columns
+// at a time, each lane solving for the range of l whose lattice point lies
+// within rmax + |w| of the origin (every hkl whose box can reach a regular g
+// is inside it), the 32 ranges flattened across the warp; candidates passing
+// the box test are queued (packed hkl) in ballot order, and whenever 32 are
+// queued every lane takes one and runs its own lookup (32 independent load
+// chains).  The UBI's plan lives in shared memory, not in registers, so that
+// three CTAs fit on an SM.
+constexpr int kQueue = 64;
+
+struct WarpPlan {
+    double u[9], ub[9], w[3];
+    float w32[3];
+    int lo[3], nh[3];
+};
+
+__device__ __forceinline__ unsigned long long pack_hkl(int h, int k, int l) {
+    return ((unsigned long long)(unsigned)(h + (1 << 20)) << 42) |
+           ((unsigned long long)(unsigned)(k + (1 << 20)) << 21) |
+           (unsigned long long)(unsigned)(l + (1 << 20));
+}
+
+__device__ __forceinline__ void unpack_hkl(unsigned long long q, double hkl[3]) {
+    hkl[0] = (double)((int)((q >> 42) & 0x1fffff) - (1 << 20));
+    hkl[1] = (double)((int)((q >> 21) & 0x1fffff) - (1 << 20));
+    hkl[2] = (double)((int)(q & 0x1fffff) - (1 << 20));
+}
+
+// Largest lane j with excl_j <= f, excl non-decreasing over lanes, excl_0 = 0.
+__device__ __forceinline__ int owner(int excl, int f) {
+    int j = 0;
+#pragma unroll
+    for (int st = 16; st > 0; st >>= 1) {
+        const int v = __shfl_sync(0xffffffffu, excl, j + st);
+        if (v <= f) j += st;
+    }
+    return j;
+}
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int& total) {
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    total = __shfl_sync(0xffffffffu, incl, 31);
+    return incl - v;
+}
+
+// Per-warp scratch for one batch of up to 32 lookups.
+struct Batch {
+    double c[32][3];
+    unsigned long long hkl[32];
+    int ix0[32], ix1[32], iy0[32], ny[32], iz0[32];
+};
+
+// The lookups of `take` queued hkl (slot = lane), warp-cooperatively: the
+// cell rows of all of them are flattened across the lanes, then the g of
+// each 32 rows, so the lanes stay converged whatever the per-query sizes.
+template <int NT>
+__device__ __forceinline__ void lookup_batch(const volatile WarpPlan* wp, Batch* bt,
+                                             const unsigned long long* q_w, int take, int lane,
+                                             const Header& H, const int* __restrict__ start,
+                                             const double* __restrict__ gs, const double* t2,
+                                             int* cnt, double* sum,
+                                             unsigned long long& tested) {
+    int nrows = 0;
+    if (lane < take) {
+        const unsigned long long q = q_w[lane];
+        double hkl[3], c[3];
+        unpack_hkl(q, hkl);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            c[r] = wp->ub[3 * r] * hkl[0] + wp->ub[3 * r + 1] * hkl[1] + wp->ub[3 * r + 2] * hkl[2];
+            bt->c[lane][r] = c[r];
+        }
+        bt->hkl[lane] = q;
+        const int iy0 = coord(c[1] - wp->w[1], H), iy1 = coord(c[1] + wp->w[1], H);
+        const int iz0 = coord(c[2] - wp->w[2], H), iz1 = coord(c[2] + wp->w[2], H);
+        bt->ix0[lane] = coord(c[0] - wp->w[0], H);
+        bt->ix1[lane] = coord(c[0] + wp->w[0], H);
+        bt->iy0[lane] = iy0;
+        bt->ny[lane] = iy1 - iy0 + 1;
+        bt->iz0[lane] = iz0;
+        nrows = (iy1 - iy0 + 1) * (iz1 - iz0 + 1);
+    }
+    __syncwarp();
+    int rtotal;
+    const int rexcl = warp_excl_scan(nrows, lane, rtotal);
+    const double w0 = wp->w[0], w1 = wp->w[1], w2 = wp->w[2];
+    for (int r0 = 0; r0 < rtotal; r0 += 32) {
+        const int rf = r0 + lane;
+        const int qj = owner(rexcl, rf);
+        const int rr = rf - __shfl_sync(0xffffffffu, rexcl, qj);
+        int st = 0, len = 0;
+        if (rf < rtotal) {
+            const int ny = bt->ny[qj];
+            const int iy = bt->iy0[qj] + rr % ny, iz = bt->iz0[qj] + rr / ny;
+            const int64_t row = ((int64_t)iz * H.nx + iy) * H.nx;
+            st = __ldg(start + row + bt->ix0[qj]);
+            len = __ldg(start + row + bt->ix1[qj] + 1) - st;
+        }
+        int gtotal;
+        const int gexcl = warp_excl_scan(len, lane, gtotal);
+        const int off = st - gexcl;
+        for (int f0 = 0; f0 < gtotal; f0 += 32) {
+            const int f = f0 + lane;
+            const int rj = owner(gexcl, f);
+            const int pos = f + __shfl_sync(0xffffffffu, off, rj);
+            const int qq = __shfl_sync(0xffffffffu, qj, rj);
+            if (f < gtotal) {
+                const double g0 = __ldg(gs + 3 * (int64_t)pos), g1 = __ldg(gs + 3 * (int64_t)pos + 1),
+                             g2 = __ldg(gs + 3 * (int64_t)pos + 2);
+                const double c0 = bt->c[qq][0], c1 = bt->c[qq][1], c2 = bt->c[qq][2];
+                if (fabs(g0 - c0) <= w0 && fabs(g1 - c1) <= w1 && fabs(g2 - c2) <= w2) {
+                    double u[9], ih[3], hkl[3];
+#pragma unroll
+                    for (int e = 0; e < 9; e++) u[e] = wp->u[e];
+                    const double sv = drlv2_exact(u, g0, g1, g2, ih);
+                    tested++;
+                    unpack_hkl(bt->hkl[qq], hkl);
+                    if (ih[0] == hkl[0] && ih[1] == hkl[1] && ih[2] == hkl[2]) {
+#pragma unroll
+                        for (int j = 0; j < NT; j++)
+                            if (sv < t2[j]) {
+                                cnt[j]++;
+                                sum[j] += sv;
+                            }
+                    }
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kGT, 2)
+k_score(const double* __restrict__ ubis, int64_t m, int parts, Header* __restrict__ Hp,
+        const int* __restrict__ start, const double* __restrict__ gs,
+        const float4* __restrict__ g4, Tols tols, int* __restrict__ pcnt,
+        double* __restrict__ psum) {
+    __shared__ unsigned long long s_q[kGT / 32][kQueue];
+    __shared__ WarpPlan s_plan[kGT / 32];
+    __shared__ Batch s_batch[kGT / 32];
+    Batch* bt = s_batch + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    unsigned long long* q_w = s_q[threadIdx.x >> 5];
+    volatile WarpPlan* wp = s_plan + (threadIdx.x >> 5);
+    const int64_t wk = ((int64_t)blockIdx.x * kGT + threadIdx.x) >> 5;
+    if (wk >= m * parts) return;  // uniform per warp
+    const int64_t i = wk / parts;
+    const int part = (int)(wk % parts);
+    const Header H = *Hp;
+    const int64_t nreg = start[H.ncells];
+    double t2[NT];
+    double tmax = 0.;
+#pragma unroll
+    for (int j = 0; j < NT; j++) {
+        tmax = fmax(tmax, tols.t[j]);
+        t2[j] = tols.t[j] * tols.t[j];
+    }
+    int cnt[NT];
+    double sum[NT];
+#pragma unroll
+    for (int j = 0; j < NT; j++) {
+        cnt[j] = 0;
+        sum[j] = 0.;
+    }
+    unsigned long long tested = 0;
+    bool ok;
+    {
+        double u[9];
+#pragma unroll
+        for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
+        const Plan P = make_plan(u, tmax, H, nreg);
+        ok = P.ok && P.nh[0] < (1 << 20) && P.nh[1] < (1 << 20) && P.nh[2] < (1 << 20);
+        if (lane == 0) {
+#pragma unroll
+            for (int e = 0; e < 9; e++) {
+                wp->u[e] = u[e];
+                wp->ub[e] = P.ub[e];
+            }
+            const double G = -H.lo;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                wp->w[r] = P.w[r];
+                wp->w32[r] = __double2float_ru(P.w[r] * (1. + 1e-6) + 1e-6 * (2. * G + P.w[r]));
+                wp->lo[r] = ok ? (int)P.lo[r] : 0;
+                wp->nh[r] = ok ? (int)P.nh[r] : 0;
+            }
+        }
+        __syncwarp();
+    }
+    if (!ok) {
+        double u[9];
+#pragma unroll
+        for (int e = 0; e < 9; e++) u[e] = wp->u[e];
+        for (int64_t f = (int64_t)part * 32 + lane; f < nreg; f += 32 * (int64_t)parts) {
+            double ih[3];
+            const double s = drlv2_exact(u, gs[3 * f], gs[3 * f + 1], gs[3 * f + 2], ih);
+            tested++;
+#pragma unroll
+            for (int j = 0; j < NT; j++)
+                if (s < t2[j]) {
+                    cnt[j]++;
+                    sum[j] += s;
+                }
+        }
+        if (part == 0 && lane == 0) atomicAdd(&Hp->nfallback, 1ull);
+    } else {
+        int qn = 0;  // queued (uniform)
+        const unsigned lt = (1u << lane) - 1u;
+        const int nh0 = wp->nh[0];
+        const int64_t nhk = (int64_t)nh0 * wp->nh[1];
+        for (int64_t hb = (int64_t)part * 32; hb < nhk; hb += 32 * (int64_t)parts) {
+            const int64_t hk = hb + lane;
+            int len = 0, l0 = 0, h = 0, k = 0;
+            if (hk < nhk) {
+                h = wp->lo[0] + (int)(hk % nh0);
+                k = wp->lo[1] + (int)(hk / nh0);
+                const double bx = wp->ub[2], by = wp->ub[5], bz = wp->ub[8];  // l direction
+                const double bb = bx * bx + by * by + bz * bz;
+                const double R = (H.rmax + sqrt(wp->w[0] * wp->w[0] + wp->w[1] * wp->w[1] +
+                                                wp->w[2] * wp->w[2])) * (1. + 1e-9) + 1e-12;
+                const double ax = wp->ub[0] * h + wp->ub[1] * k,
+                             ay = wp->ub[3] * h + wp->ub[4] * k,
+                             az = wp->ub[6] * h + wp->ub[7] * k;
+                const double ab = ax * bx + ay * by + az * bz;
+                const double aa = ax * ax + ay * ay + az * az;
+                const double disc = ab * ab - bb * (aa - R * R);
+                if (disc >= 0.) {
+                    const double sq = sqrt(disc);
+                    const double la = fmax(floor((-ab - sq) / bb) - 1., (double)wp->lo[2]);
+                    const double lb = fmin(ceil((-ab + sq) / bb) + 1.,
+                                           (double)(wp->lo[2] + wp->nh[2] - 1));
+                    if (la <= lb) {
+                        l0 = (int)la;
+                        len = (int)(lb - la) + 1;
+                    }
+                }
+            }
+            int incl = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int excl = incl - len;
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                const int f = f0 + lane;
+                int j = 0;  // largest lane j with excl_j <= f
+#pragma unroll
+                for (int st = 16; st > 0; st >>= 1) {
+                    const int v = __shfl_sync(0xffffffffu, excl, j + st);
+                    if (v <= f) j += st;
+                }
+                const int hj = __shfl_sync(0xffffffffu, h, j);
+                const int kj = __shfl_sync(0xffffffffu, k, j);
+                const int lj = __shfl_sync(0xffffffffu, l0, j) + f -
+                               __shfl_sync(0xffffffffu, excl, j);
+                bool pass = false;
+                if (f < total) {
+                    const double hkl[3] = {(double)hj, (double)kj, (double)lj};
+                    double c[3];
+                    bool in = true;
+                    double d2 = 0.;
+                    const double G = -H.lo;
+#pragma unroll
+                    for (int r = 0; r < 3; r++) {
+                        c[r] = wp->ub[3 * r] * hkl[0] + wp->ub[3 * r + 1] * hkl[1] +
+                               wp->ub[3 * r + 2] * hkl[2];
+                        const double wr = wp->w[r];
+                        in = in && (c[r] - wr <= G) && (c[r] + wr >= -G);
+                        const double e = fmax(fabs(c[r]) - wr, 0.);
+                        d2 += e * e;
+                    }
+                    pass = in && d2 <= H.rmax * H.rmax * (1. + 1e-9);
+                }
+                const unsigned mask = __ballot_sync(0xffffffffu, pass);
+                if (pass) q_w[qn + __popc(mask & lt)] = pack_hkl(hj, kj, lj);
+                qn += __popc(mask);
+                __syncwarp();
+                if (qn >= 32) {
+                    lookup_batch<NT>(wp, bt, q_w, 32, lane, H, start, gs, t2, cnt, sum, tested);
+                    const int rest = qn - 32;
+                    unsigned long long v = 0;
+                    if (lane < rest) v = q_w[32 + lane];
+                    __syncwarp();
+                    if (lane < rest) q_w[lane] = v;
+                    __syncwarp();
+                    qn = rest;
+                }
+            }
+        }
+        if (qn > 0) lookup_batch<NT>(wp, bt, q_w, qn, lane, H, start, gs, t2, cnt, sum, tested);
+    }
+#pragma unroll
+    for (int j = 0; j < NT; j++) {
+        const int cs = warp_sum(cnt[j]);
+        const double ss = warp_sum(sum[j]);
+        if (lane == 0) {
+            pcnt[(i * parts + part) * NT + j] = cs;
+            psum[(i * parts + part) * NT + j] = ss;
+        }
+    }
+    const long long tt = warp_sum((long long)tested);
+    if (lane == 0 && tt) atomicAdd(&Hp->ntested, (unsigned long long)tt);
+}
+
+// One thread per UBI: CTA-part partials in a fixed order, then the g-vectors
+// outside the regular range, one by one in list order.
+__global__ void __launch_bounds__(kGT)
+k_score_finish(const double* __restrict__ ubis, int64_t m, int parts, int ntol, Tols tols,
+               const int* __restrict__ pcnt, const double* __restrict__ psum,
+               const double* __restrict__ gv, const int* __restrict__ special,
+               const int* __restrict__ nspecial, int* __restrict__ counts,
+               double* __restrict__ sums) {
+    const int64_t i = (int64_t)blockIdx.x * kGT + threadIdx.x;
+    if (i >= m) return;
+    int c[ID11B_MAX_TOLS] = {0, 0, 0, 0};
+    double s[ID11B_MAX_TOLS] = {0., 0., 0., 0.};
+    for (int p = 0; p < parts; p++)
+        for (int j = 0; j < ntol; j++) {
+            c[j] += pcnt[(i * parts + p) * ntol + j];
+            s[j] += psum[(i * parts + p) * ntol + j];
+        }
+    const int ns = *nspecial;
+    if (ns) {
+        double u[9];
+        for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
+        for (int q = 0; q < ns; q++) {
+            const int64_t k = special[q];
+            double ih[3];
+            const double v = drlv2_exact(u, gv[3 * k], gv[3 * k + 1], gv[3 * k + 2], ih);
+            for (int j = 0; j < ntol; j++)
+                if (v < tols.t[j] * tols.t[j]) {
+                    c[j]++;
+                    s[j] += v;
+                }
+        }
+    }
+    for (int j = 0; j < ntol; j++) {
+        counts[i * ntol + j] = c[j];
+        if (sums) sums[i * ntol + j] = s[j];
+    }
+}
+
+}  // namespace grid
+}  // namespace id11b
+
+namespace id11b {
+namespace grid {
+
+static int num_sms() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 148;
+}
+
+static unsigned grid_for(int64_t items, int per) {
+    int64_t b = (items + per - 1) / per;
+    int64_t cap = (int64_t)num_sms() * 8;
+    if (b > cap) b = cap;
+    return (unsigned)(b > 0 ? b : 1);
+}
+
+// exclusive scan of x[0..len) into y (len >= 1), tot: scratch
+static int scan(const int* x, int64_t len, int* y, int* tot, cudaStream_t st) {
+    const int64_t nb = (len + kScanPer - 1) / kScanPer;
+    k_scan_local<<<(unsigned)nb, kScanT, 0, st>>>(x, len, y, tot);
+    ID11B_CHECK_LAUNCH();
+    k_scan_totals<<<1, kScanT, 0, st>>>(tot, (int)nb);
+    ID11B_CHECK_LAUNCH();
+    k_scan_add<<<(unsigned)nb, kScanT, 0, st>>>(y, len, tot);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+// work items (warps) per UBI: enough warps for ~4 waves of 8 warps x 8 CTAs per SM
+static int score_parts(int64_t m) {
+    if (m <= 0) return 1;
+    int64_t want = (int64_t)num_sms() * 64 * 4;
+    int64_t p = (want + m - 1) / m;
+    if (p > kMaxParts) p = kMaxParts;
+    return (int)(p < 1 ? 1 : p);
+}
+
+}  // namespace grid
+}  // namespace id11b
+
+using namespace id11b::grid;
+
+extern "C" int id11b_dev_gvec_bounds(const double* gv, int64_t n, uint32_t* bounds, void* stream) {
+    if (n < 0 || !bounds || (n > 0 && !gv)) return ID11B_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    ID11B_CHECK(cudaMemsetAsync(bounds, 0, 2 * sizeof(uint32_t), st));
+    if (n == 0) return ID11B_OK;
+    k_bounds<<<grid_for(n, kGT), kGT, 0, st>>>(gv, n, bounds);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+extern "C" int id11b_grid_plan(float gmax, int64_t n, double cell, int32_t* nx, double* cs) {
+    if (!nx || !cs || n < 0 || !(gmax >= 0.f) || !(cell >= 0.)) return ID11B_ERR_ARG;
+    const double G = (double)gmax * (1. + 1e-6) + 1e-300;
+    double c = cell;
+    if (c == 0.) c = 2. * G / fmax(1., cbrt((double)n));  // ~one g per cell of the cube
+    int64_t k = (int64_t)ceil(2. * G / c);
+    if (k < 1) k = 1;
+    if (k > 400) {  // at most 6.4e7 cells
+        k = 400;
+    }
+    *nx = (int32_t)k;
+    *cs = fmax(c, 2. * G / (double)k);
+    return ID11B_OK;
+}
+
+extern "C" int64_t id11b_grid_bytes(int64_t n, int32_t nx) {
+    if (n < 0 || nx < 1) return -1;
+    return (int64_t)layout(n, (int64_t)nx * nx * nx).bytes;
+}
+
+extern "C" int id11b_dev_build_grid(const double* gv, int64_t n, float gmax, float rmax, double cs,
+                                    int32_t nx, void* gridbuf, int64_t grid_bytes, void* stream) {
+    if (n < 0 || nx < 1 || nx > 400 || !gridbuf || (n > 0 && !gv) || !(cs > 0.) ||
+        !(gmax >= 0.f) || !(rmax >= 0.f))
+        return ID11B_ERR_ARG;
+    if ((uintptr_t)gridbuf & 255) return ID11B_ERR_ALIGN;
+    if (n > INT32_MAX - 1) return ID11B_ERR_SIZE;
+    const int64_t ncells = (int64_t)nx * nx * nx;
+    const Layout L = layout(n, ncells);
+    if (grid_bytes < (int64_t)L.bytes) return ID11B_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    char* b = (char*)gridbuf;
+    Header h;
+    memset(&h, 0, sizeof(h));
+    h.lo = -((double)gmax * (1. + 1e-6) + 1e-300);
+    h.cs = cs;
+    h.inv_cs = 1.0 / cs;
+    h.rmax = (double)rmax;
+    h.ncells = ncells;
+    h.n = n;
+    h.nx = nx;
+    static_assert(sizeof(Header) <= 256, "header");
+    // a copy from pageable memory returns once the source has been staged,
+    // so the stack value may go out of scope
+    ID11B_CHECK(cudaMemcpyAsync(b + L.header, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+    int* cnt = (int*)(b + L.cnt);
+    int* start = (int*)(b + L.start);
+    int* flag = (int*)(b + L.flag);
+    int* spos = (int*)(b + L.spos);
+    int* tot = (int*)(b + L.tot);
+    ID11B_CHECK(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(ncells + 1), st));
+    ID11B_CHECK(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)(n + 1), st));
+    const Header* H = (const Header*)(b + L.header);
+    if (n > 0) {
+        k_count<<<grid_for(n, kGT), kGT, 0, st>>>(gv, n, H, cnt, flag);
+        ID11B_CHECK_LAUNCH();
+    }
+    int rc = scan(cnt, ncells + 1, start, tot, st);
+    if (rc) return rc;
+    rc = scan(flag, n + 1, spos, tot, st);
+    if (rc) return rc;
+    ID11B_CHECK(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(ncells + 1), st));  // cursors
+    if (n > 0) {
+        k_scatter<<<grid_for(n, kGT), kGT, 0, st>>>(gv, n, H, start, cnt, (double*)(b + L.g),
+                                                    (int*)(b + L.idx), spos, (int*)(b + L.spec));
+        ID11B_CHECK_LAUNCH();
+        k_sort_cells<<<grid_for(ncells, kGT), kGT, 0, st>>>(start, ncells, (double*)(b + L.g),
+                                                            (int*)(b + L.idx),
+                                                            (float4*)(b + L.g4));
+        ID11B_CHECK_LAUNCH();
+    }
+    return ID11B_OK;
+}
+
+extern "C" int64_t id11b_grid_score_workspace_bytes(int64_t m, int ntol) {
+    if (m < 0 || ntol < 1 || ntol > ID11B_MAX_TOLS) return -1;
+    const int64_t items = (m > 0 ? m : 1) * score_parts(m) * ntol;
+    return (int64_t)(al256(sizeof(int) * (size_t)items) + al256(sizeof(double) * (size_t)items));
+}
+
+extern "C" int id11b_dev_score_grid(const double* ubis, int64_t m, const double* gv, int64_t n,
+                                    int32_t nx, const void* gridbuf, const double* tols_host,
+                                    int ntol, int32_t* counts, double* sums, void* ws,
+                                    int64_t ws_bytes, void* stream) {
+    if (!tols_host || ntol < 1 || ntol > ID11B_MAX_TOLS || m < 0 || n < 0 || nx < 1 ||
+        nx > 400 || !gridbuf || !ws || (m > 0 && (!ubis || !counts)) || (n > 0 && !gv))
+        return ID11B_ERR_ARG;
+    Tols T;
+    for (int j = 0; j < ID11B_MAX_TOLS; j++) T.t[j] = j < ntol ? tols_host[j] : 0.;
+    for (int j = 0; j < ntol; j++)
+        if (!(tols_host[j] >= 0.) || !(tols_host[j] < 1e3)) return ID11B_ERR_ARG;
+    if (((uintptr_t)gridbuf & 255) || ((uintptr_t)ws & 255)) return ID11B_ERR_ALIGN;
+    if (ws_bytes < id11b_grid_score_workspace_bytes(m, ntol)) return ID11B_ERR_SIZE;
+    if (m > INT32_MAX) return ID11B_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    const Layout L = layout(n, (int64_t)nx * nx * nx);
+    char* b = (char*)gridbuf;
+    Header* H = (Header*)b;
+    ID11B_CHECK(cudaMemsetAsync(&H->nfallback, 0, 2 * sizeof(unsigned long long), st));
+    if (m == 0) return ID11B_OK;
+    const int parts = score_parts(m);
+    const int64_t items = m * parts * ntol;
+    int* pcnt = (int*)ws;
+    double* psum = (double*)((char*)ws + al256(sizeof(int) * (size_t)items));
+    const int64_t warps = m * parts;
+    const unsigned blocks = (unsigned)((warps * 32 + kGT - 1) / kGT);
+    const int* start = (const int*)(b + L.start);
+    const double* gs = (const double*)(b + L.g);
+    const float4* g4 = (const float4*)(b + L.g4);
+    switch (ntol) {
+        case 1: k_score<1><<<blocks, kGT, 0, st>>>(ubis, m, parts, H, start, gs, g4, T, pcnt, psum); break;
+        case 2: k_score<2><<<blocks, kGT, 0, st>>>(ubis, m, parts, H, start, gs, g4, T, pcnt, psum); break;
+        case 3: k_score<3><<<blocks, kGT, 0, st>>>(ubis, m, parts, H, start, gs, g4, T, pcnt, psum); break;
+        default: k_score<4><<<blocks, kGT, 0, st>>>(ubis, m, parts, H, start, gs, g4, T, pcnt, psum); break;
+    }
+    ID11B_CHECK_LAUNCH();
+    k_score_finish<<<(unsigned)((m + kGT - 1) / kGT), kGT, 0, st>>>(
+        ubis, m, parts, ntol, T, pcnt, psum, gv, (const int*)(b + L.spec),
+        (const int*)(b + L.spos) + n, counts, sums);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+extern "C" int id11b_grid_stats(const void* gridbuf, int64_t* nregular, int64_t* nspecial,
+                                int64_t* nfallback, int64_t* ntested, void* stream) {
+    if (!gridbuf) return ID11B_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    Header h;
+    ID11B_CHECK(cudaMemcpyAsync(&h, gridbuf, sizeof(h), cudaMemcpyDeviceToHost, st));
+    ID11B_CHECK(cudaStreamSynchronize(st));
+    const Layout L = layout(h.n, h.ncells);
+    int nr = 0, ns = 0;
+    ID11B_CHECK(cudaMemcpyAsync(&nr, (const char*)gridbuf + L.start + sizeof(int) * h.ncells,
+                                sizeof(int), cudaMemcpyDeviceToHost, st));
+    ID11B_CHECK(cudaMemcpyAsync(&ns, (const char*)gridbuf + L.spos + sizeof(int) * h.n,
+                                sizeof(int), cudaMemcpyDeviceToHost, st));
+    ID11B_CHECK(cudaStreamSynchronize(st));
+    if (nregular) *nregular = nr;
+    if (nspecial) *nspecial = ns;
+    if (nfallback) *nfallback = (int64_t)h.nfallback;
+    if (ntested) *ntested = (int64_t)h.ntested;
+    return ID11B_OK;
+}

@@ -216,6 +216,39 @@ int id11b_dev_score_batch_tiled(const double *ubis, int64_t m, const double *gv,
                                 double *sums, int ubis_per_thread, int gsplit, void *ws,
                                 int64_t ws_bytes, void *stream);
 
+/* Reciprocal-space cell index (no reference counterpart; it replaces the
+ * reference's test of every g against every UBI in score(), ImageD11
+ * src/closest.c:227-248, with a lookup of the g near each UB.hkl).
+ * Regular g-vectors (finite, every |g_j| <= 1024) are binned into nx^3 cubic
+ * cells of side cs over [-gmax, gmax]^3, sorted by cell (x fastest; within a
+ * cell by index); the others are kept in an index list.
+ *   1. id11b_dev_gvec_bounds: bounds[0] = max |g_j|, bounds[1] = max |g| over
+ *      regular g, as float bits rounded up (device, 2 x uint32);
+ *   2. id11b_grid_plan (host): nx and cs for n g-vectors; cell = 0 picks about
+ *      one g per cell of the cube, else the requested side (nx <= 400);
+ *   3. id11b_dev_build_grid into gridbuf (id11b_grid_bytes(n, nx), 256-byte
+ *      aligned).
+ * id11b_dev_score_grid then gives the counts (and optional sums of drlv2) of
+ * id11b_dev_score_batch, identical to the reference's score() for every
+ * (UBI, tol): every candidate pair is evaluated in the reference's FP64
+ * arithmetic.  A UBI whose lookup would cost more than a plain scan
+ * (non-finite, singular, condition number above 1e6, more candidate hkl
+ * than g) is scored by a plain scan.  id11b_grid_stats reports the regular and
+ * listed g, and for the last score call the UBIs scanned plainly and the pairs
+ * evaluated. */
+int id11b_dev_gvec_bounds(const double *gv, int64_t n, uint32_t *bounds, void *stream);
+int id11b_grid_plan(float gmax, int64_t n, double cell, int32_t *nx, double *cs);
+int64_t id11b_grid_bytes(int64_t n, int32_t nx);
+int id11b_dev_build_grid(const double *gv, int64_t n, float gmax, float rmax, double cs,
+                         int32_t nx, void *gridbuf, int64_t grid_bytes, void *stream);
+int64_t id11b_grid_score_workspace_bytes(int64_t m, int ntol);
+int id11b_dev_score_grid(const double *ubis, int64_t m, const double *gv, int64_t n, int32_t nx,
+                         const void *gridbuf, const double *tols_host, int ntol,
+                         int32_t *counts, double *sums, void *ws, int64_t ws_bytes,
+                         void *stream);
+int id11b_grid_stats(const void *gridbuf, int64_t *nregular, int64_t *nspecial,
+                     int64_t *nfallback, int64_t *ntested, void *stream);
+
 /* `iters` rounds of score_and_refine (ImageD11 src/closest.c:267-345) for each
  * of m UBIs against all n g-vectors, ubis (m,3,3) updated in place; npk and
  * mean_drlv2 (optional) receive the last round's count and mean drlv2.

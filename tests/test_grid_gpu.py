@@ -1,0 +1,114 @@
+"""Scoring through the reciprocal-space cell index vs the oracle and the
+golden vectors.
+
+Counts are bit-exact: every candidate pair is evaluated in the reference's
+FP64 arithmetic and the lookup boxes are conservative, so the counted set is
+the reference's.  Sums of drlv2 are FP64 sums in another order than the
+reference's loop: 1e-12 relative."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SUM_RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def B():
+    from imaged11_b200 import batch
+    return batch
+
+
+@pytest.fixture(scope="module")
+def scene():
+    from imaged11_b200 import synth
+    ps = synth.simulate(120, "Al", gmax=1.3, seed=31, noise_frac=0.10)
+    rng = np.random.default_rng(32)
+    ubis = synth.trial_ubis(ps.ubis, 1500, 0.1, 0.5, rng)
+    return ps, ubis
+
+
+def test_golden_counts(B, golden, cuda):
+    d = golden["scoring"]
+    grid = B.GvecGrid(d["sc_gv"])
+    c = B.score_grid(d["sc_ubis"], grid, d["sc_tols"]).cpu().numpy()
+    assert np.array_equal(c, d["sc_counts"])
+
+
+def test_adversarial_and_special_g(B, golden, oracle, cuda):
+    d = golden["scoring"]
+    grid = B.GvecGrid(d["adv_gv"])
+    st = grid.stats()
+    assert st["regular"] + st["special"] == len(d["adv_gv"])
+    ubis = np.concatenate([d["adv_ubi"][None], d["sc_ubis"][:7]])
+    c = B.score_grid(ubis, grid, d["sc_tols"]).cpu().numpy()
+    assert np.array_equal(c[0], d["adv_counts"])
+    assert np.array_equal(c, oracle.score_many(ubis, d["adv_gv"], d["sc_tols"]))
+
+
+def test_scene_counts_and_sums(B, oracle, scene, cuda):
+    ps, ubis = scene
+    tols = [0.02, 0.05, 0.1]
+    grid = B.GvecGrid(ps.gv)
+    c, s = B.score_grid(ubis, grid, tols, sums=True)
+    c = c.cpu().numpy()
+    s = s.cpu().numpy()
+    assert np.array_equal(c, oracle.score_many(ubis, ps.gv, tols))
+    st = grid.stats()
+    assert st["fallback_ubis"] == 0
+    assert st["pairs_tested"] < 0.05 * len(ubis) * len(ps.gv)   # the point of the index
+    for i in range(0, len(ubis), 37):
+        for j, t in enumerate(tols):
+            n, mean, _ = oracle.score_and_refine(ubis[i], ps.gv, t)
+            assert n == c[i, j]
+            assert abs(s[i, j] - mean * n) <= SUM_RTOL * mean * n + 1e-300
+    # deterministic: the same sums bit for bit
+    c2, s2 = B.score_grid(ubis, grid, tols, sums=True)
+    assert np.array_equal(s2.cpu().numpy(), s)
+
+
+@pytest.mark.parametrize("cell", [0.004, 0.03, 0.25, 1.0])
+def test_cell_sizes(B, oracle, scene, cell, cuda):
+    ps, ubis = scene
+    u = ubis[:300]
+    grid = B.GvecGrid(ps.gv, cell=cell)
+    c = B.score_grid(u, grid, [0.05, 0.1]).cpu().numpy()
+    assert np.array_equal(c, oracle.score_many(u, ps.gv, [0.05, 0.1])), cell
+
+
+def test_ragged_and_empty(B, oracle, scene, cuda):
+    ps, ubis = scene
+    for m, n in [(1, 1), (1, 1023), (3, 1025), (1025, 777), (257, 5000)]:
+        g = ps.gv[:n]
+        u = ubis[:m]
+        c = B.score_grid(u, B.GvecGrid(g), [0.05, 0.1]).cpu().numpy()
+        assert np.array_equal(c, oracle.score_many(u, g, [0.05, 0.1])), (m, n)
+    c = B.score_grid(np.eye(3)[None] * 4.05, B.GvecGrid(np.zeros((0, 3))), [0.1]).cpu().numpy()
+    assert c.shape == (1, 1) and c[0, 0] == 0
+    c = B.score_grid(np.zeros((0, 3, 3)), B.GvecGrid(np.ones((10, 3))), [0.1])
+    assert c.shape == (0, 1)
+
+
+def test_plain_scan_ubis_and_large_tols(B, oracle, scene, cuda):
+    ps, ubis = scene
+    g = ps.gv[:20000]
+    u = ubis[:40].copy()
+    u[3] *= 1e5                      # many more candidate hkl than g
+    u[5, 1, 1] = np.nan              # non-finite
+    u[7] = 0.0                       # singular: every g has h = 0
+    u[9] = np.diag([1e4, 1.0, 1e-4]) # condition number 1e8
+    grid = B.GvecGrid(g)
+    c = B.score_grid(u, grid, [0.05, 0.1]).cpu().numpy()
+    assert np.array_equal(c, oracle.score_many(u, g, [0.05, 0.1]))
+    assert grid.stats()["fallback_ubis"] == 4
+    for tols in ([0.1, 0.47], [0.5, 0.9], [3.0]):
+        c = B.score_grid(u, grid, tols).cpu().numpy()
+        assert np.array_equal(c, oracle.score_many(u, g, tols)), tols
+
+
+def test_matches_score_batch(B, scene, cuda):
+    ps, ubis = scene
+    tols = [0.01, 0.03, 0.07, 0.2]
+    a = B.score_grid(ubis, B.GvecGrid(ps.gv), tols).cpu().numpy()
+    b = B.score_batch(ubis, B.GvecSet(ps.gv), tols).cpu().numpy()
+    assert np.array_equal(a, b)

@@ -30,7 +30,20 @@
 namespace id11b {
 namespace grid {
 
-constexpr int kGT = 256;           // threads per CTA (8 warps, one warp per work item)
+constexpr int kGT = 256;           // threads per CTA of the build kernels
+// scoring CTAs: warps (one per work item) and the resident CTAs per SM the
+// register budget is compiled for.  Occupancy decides the speed of the
+// latency-bound lookups: 20,000 UBIs x 1.1M g on B200 took 13.0 ms at 8 warps
+// x 2 CTAs (107 registers), 9.9 ms at 8 x 3, 9.5 ms at 2 x 12, 9.4 ms at
+// 1 x 24 (80 registers) and 8.0 ms at 1 x 32 (64 registers, a few spilled).
+#ifndef ID11B_GRID_WARPS
+#define ID11B_GRID_WARPS 1
+#endif
+#ifndef ID11B_GRID_MINB
+#define ID11B_GRID_MINB 32
+#endif
+constexpr int kSW = ID11B_GRID_WARPS;
+constexpr int kST = 32 * kSW;
 constexpr int kScanT = 1024;       // scan CTA
 constexpr int kScanPer = 4 * kScanT;
 constexpr double kGLimit = 1024.0;  // regular g: finite, every |g_j| <= 1024
@@ -55,10 +68,10 @@ struct Tols {
 
 __host__ __device__ inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Grid buffer: header | cnt[ncells+1] | start[ncells+1] | g[n][3] | g4[n] | gidx[n] |
+// Grid buffer: header | cnt[ncells+1] | start[ncells+1] | g[n][3] | gidx[n] |
 // flag[n+1] | spos[n+1] | spec[n] | scan totals
 struct Layout {
-    size_t header, cnt, start, g, g4, idx, flag, spos, spec, tot, bytes;
+    size_t header, cnt, start, g, idx, flag, spos, spec, tot, bytes;
 };
 
 __host__ __device__ inline Layout layout(int64_t n, int64_t ncells) {
@@ -70,7 +83,6 @@ __host__ __device__ inline Layout layout(int64_t n, int64_t ncells) {
     L.cnt = o;    o = al256(o + sizeof(int) * (size_t)(ncells + 1));
     L.start = o;  o = al256(o + sizeof(int) * (size_t)(ncells + 1));
     L.g = o;      o = al256(o + sizeof(double) * 3 * nn);
-    L.g4 = o;     o = al256(o + sizeof(float4) * nn);
     L.idx = o;    o = al256(o + sizeof(int) * nn);
     L.flag = o;   o = al256(o + sizeof(int) * (nn + 1));
     L.spos = o;   o = al256(o + sizeof(int) * (nn + 1));
@@ -243,7 +255,7 @@ k_scatter(const double* __restrict__ gv, int64_t n, const Header* __restrict__ H
 // result, does not depend on the order the scatter's atomics ran in
 __global__ void __launch_bounds__(kGT)
 k_sort_cells(const int* __restrict__ start, int64_t ncells, double* __restrict__ gs,
-             int* __restrict__ gidx, float4* __restrict__ g4) {
+             int* __restrict__ gidx) {
     for (int64_t c = (int64_t)blockIdx.x * kGT + threadIdx.x; c < ncells;
          c += (int64_t)gridDim.x * kGT) {
         const int a = start[c], b = start[c + 1];
@@ -264,9 +276,6 @@ k_sort_cells(const int* __restrict__ start, int64_t ncells, double* __restrict__
             gs[3 * (int64_t)j + 4] = y;
             gs[3 * (int64_t)j + 5] = z;
         }
-        for (int i = a; i < b; i++)
-            g4[i] = make_float4((float)gs[3 * (int64_t)i], (float)gs[3 * (int64_t)i + 1],
-                                (float)gs[3 * (int64_t)i + 2], 0.f);
     }
 }
 
@@ -331,81 +340,17 @@ __device__ __forceinline__ Plan make_plan(const double u[9], double tmax, const 
     return P;
 }
 
-__device__ __forceinline__ void hkl_of(const Plan& P, int64_t q, double hkl[3]) {
-    const int64_t i0 = q % P.nh[0], rest = q / P.nh[0];
-    const int64_t i1 = rest % P.nh[1], i2 = rest / P.nh[1];
-    hkl[0] = (double)(P.lo[0] + i0);
-    hkl[1] = (double)(P.lo[1] + i1);
-    hkl[2] = (double)(P.lo[2] + i2);
-}
-
-__device__ __forceinline__ void centre(const Plan& P, const double hkl[3], double c[3]) {
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-        c[r] = P.ub[3 * r] * hkl[0] + P.ub[3 * r + 1] * hkl[1] + P.ub[3 * r + 2] * hkl[2];
-}
-
-// can the box around c reach a regular g?
-__device__ __forceinline__ bool reaches(const Plan& P, const double c[3], const Header& H) {
-    const double G = -H.lo;
-    bool in = true;
-    double d2 = 0.;
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-        in = in && (c[r] - P.w[r] <= G) && (c[r] + P.w[r] >= -G);
-        // distance from the origin to the nearest point of the box, per axis
-        const double e = fmax(fabs(c[r]) - P.w[r], 0.);
-        d2 += e * e;
-    }
-    return in && d2 <= H.rmax * H.rmax * (1. + 1e-9);
-}
-
-// Visit the g inside the box around c (one lane, one hkl): fn(pos, g0, g1, g2).
-// Rows of cells along x are contiguous ranges of the cell-sorted g.  The FP32
-// copy filters first with half-widths w32 widened past every FP32 rounding
-// (so it never rejects a g of the FP64 box); the FP64 box test follows.
-template <class Fn>
-__device__ __forceinline__ void visit_box(const double c[3], const double w[3],
-                                          const float w32[3], const Header& H,
-                                          const int* __restrict__ start,
-                                          const double* __restrict__ gs,
-                                          const float4* __restrict__ g4, Fn&& fn) {
-    const int ix0 = coord(c[0] - w[0], H), ix1 = coord(c[0] + w[0], H);
-    const int iy0 = coord(c[1] - w[1], H), iy1 = coord(c[1] + w[1], H);
-    const int iz0 = coord(c[2] - w[2], H), iz1 = coord(c[2] + w[2], H);
-    const float cx = (float)c[0], cy = (float)c[1], cz = (float)c[2];
-    for (int iz = iz0; iz <= iz1; iz++)
-        for (int iy = iy0; iy <= iy1; iy++) {
-            const int64_t row = ((int64_t)iz * H.nx + iy) * H.nx;
-            const int st = __ldg(start + row + ix0), en = __ldg(start + row + ix1 + 1);
-            for (int p = st; p < en; p++) {
-                const float4 v = __ldg(g4 + p);
-                if (fabsf(v.x - cx) <= w32[0] && fabsf(v.y - cy) <= w32[1] &&
-                    fabsf(v.z - cz) <= w32[2]) {
-                    const double g0 = __ldg(gs + 3 * (int64_t)p),
-                                 g1 = __ldg(gs + 3 * (int64_t)p + 1),
-                                 g2 = __ldg(gs + 3 * (int64_t)p + 2);
-                    if (fabs(g0 - c[0]) <= w[0] && fabs(g1 - c[1]) <= w[1] &&
-                        fabs(g2 - c[2]) <= w[2])
-                        fn(p, g0, g1, g2);
-                }
-            }
-        }
-}
-
 // Per-warp queue of hkl that reach the data.  Enumeration: 32 (h, k) columns
 // at a time, each lane solving for the range of l whose lattice point lies
 // within rmax + |w| of the origin (every hkl whose box can reach a regular g
 // is inside it), the 32 ranges flattened across the warp; candidates passing
 // the box test are queued (packed hkl) in ballot order, and whenever 32 are
-// queued every lane takes one and runs its own lookup (32 independent load
-// chains).  The UBI's plan lives in shared memory, not in registers, so that
-// three CTAs fit on an SM.
+// queued the warp runs the 32 lookups together (lookup_batch).  The UBI's plan
+// lives in shared memory, not in registers.
 constexpr int kQueue = 64;
 
 struct WarpPlan {
     double u[9], ub[9], w[3];
-    float w32[3];
     int lo[3], nh[3];
 };
 
@@ -531,19 +476,19 @@ __device__ __forceinline__ void lookup_batch(const volatile WarpPlan* wp, Batch*
 }
 
 template <int NT>
-__global__ void __launch_bounds__(kGT, 2)
+__global__ void __launch_bounds__(kST, ID11B_GRID_MINB)
 k_score(const double* __restrict__ ubis, int64_t m, int parts, Header* __restrict__ Hp,
         const int* __restrict__ start, const double* __restrict__ gs,
-        const float4* __restrict__ g4, Tols tols, int* __restrict__ pcnt,
+        Tols tols, int* __restrict__ pcnt,
         double* __restrict__ psum) {
-    __shared__ unsigned long long s_q[kGT / 32][kQueue];
-    __shared__ WarpPlan s_plan[kGT / 32];
-    __shared__ Batch s_batch[kGT / 32];
+    __shared__ unsigned long long s_q[kSW][kQueue];
+    __shared__ WarpPlan s_plan[kSW];
+    __shared__ Batch s_batch[kSW];
     Batch* bt = s_batch + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     unsigned long long* q_w = s_q[threadIdx.x >> 5];
     volatile WarpPlan* wp = s_plan + (threadIdx.x >> 5);
-    const int64_t wk = ((int64_t)blockIdx.x * kGT + threadIdx.x) >> 5;
+    const int64_t wk = ((int64_t)blockIdx.x * kST + threadIdx.x) >> 5;
     if (wk >= m * parts) return;  // uniform per warp
     const int64_t i = wk / parts;
     const int part = (int)(wk % parts);
@@ -577,11 +522,9 @@ k_score(const double* __restrict__ ubis, int64_t m, int parts, Header* __restric
                 wp->u[e] = u[e];
                 wp->ub[e] = P.ub[e];
             }
-            const double G = -H.lo;
 #pragma unroll
             for (int r = 0; r < 3; r++) {
                 wp->w[r] = P.w[r];
-                wp->w32[r] = __double2float_ru(P.w[r] * (1. + 1e-6) + 1e-6 * (2. * G + P.w[r]));
                 wp->lo[r] = ok ? (int)P.lo[r] : 0;
                 wp->nh[r] = ok ? (int)P.nh[r] : 0;
             }
@@ -866,8 +809,7 @@ extern "C" int id11b_dev_build_grid(const double* gv, int64_t n, float gmax, flo
                                                     (int*)(b + L.idx), spos, (int*)(b + L.spec));
         ID11B_CHECK_LAUNCH();
         k_sort_cells<<<grid_for(ncells, kGT), kGT, 0, st>>>(start, ncells, (double*)(b + L.g),
-                                                            (int*)(b + L.idx),
-                                                            (float4*)(b + L.g4));
+                                                            (int*)(b + L.idx));
         ID11B_CHECK_LAUNCH();
     }
     return ID11B_OK;
@@ -904,15 +846,14 @@ extern "C" int id11b_dev_score_grid(const double* ubis, int64_t m, const double*
     int* pcnt = (int*)ws;
     double* psum = (double*)((char*)ws + al256(sizeof(int) * (size_t)items));
     const int64_t warps = m * parts;
-    const unsigned blocks = (unsigned)((warps * 32 + kGT - 1) / kGT);
+    const unsigned blocks = (unsigned)((warps + kSW - 1) / kSW);
     const int* start = (const int*)(b + L.start);
     const double* gs = (const double*)(b + L.g);
-    const float4* g4 = (const float4*)(b + L.g4);
     switch (ntol) {
-        case 1: k_score<1><<<blocks, kGT, 0, st>>>(ubis, m, parts, H, start, gs, g4, T, pcnt, psum); break;
-        case 2: k_score<2><<<blocks, kGT, 0, st>>>(ubis, m, parts, H, start, gs, g4, T, pcnt, psum); break;
-        case 3: k_score<3><<<blocks, kGT, 0, st>>>(ubis, m, parts, H, start, gs, g4, T, pcnt, psum); break;
-        default: k_score<4><<<blocks, kGT, 0, st>>>(ubis, m, parts, H, start, gs, g4, T, pcnt, psum); break;
+        case 1: k_score<1><<<blocks, kST, 0, st>>>(ubis, m, parts, H, start, gs, T, pcnt, psum); break;
+        case 2: k_score<2><<<blocks, kST, 0, st>>>(ubis, m, parts, H, start, gs, T, pcnt, psum); break;
+        case 3: k_score<3><<<blocks, kST, 0, st>>>(ubis, m, parts, H, start, gs, T, pcnt, psum); break;
+        default: k_score<4><<<blocks, kST, 0, st>>>(ubis, m, parts, H, start, gs, T, pcnt, psum); break;
     }
     ID11B_CHECK_LAUNCH();
     k_score_finish<<<(unsigned)((m + kGT - 1) / kGT), kGT, 0, st>>>(

@@ -96,7 +96,36 @@ def grid_measure(torch, dev, ps, ubis, steps=5, flush=None, check_counts=None, c
     times = cuda_time_ms(torch, run, steps, flush)
     ms = float(np.mean(times))
     st = grid.stats()
+
+    # batched score_and_assign (the fight_over_peaks loop, tol 0.05) against
+    # the drop-in kernel called once per grain, on the first 256 UBIs
+    d = torch.empty(n, dtype=torch.float64, device=dev)
+    lab = torch.empty(n, dtype=torch.int32, device=dev)
+    one = torch.empty(1, dtype=torch.int32, device=dev)
+
+    def assign(k):
+        d.fill_(2.0)
+        lab.fill_(-1)
+        batch.score_and_assign_grid(ubis_d[:k], grid, 0.05, d, lab)
+
+    def assign_seq(k):
+        d.fill_(2.0)
+        lab.fill_(-1)
+        for i in range(k):
+            batch.lib.id11b_dev_score_and_assign(ubis_d[i].data_ptr(), gv_d.data_ptr(), 0.05,
+                                                 d.data_ptr(), lab.data_ptr(), i, n,
+                                                 one.data_ptr(), None)
+    k = min(256, m)
+    assign_seq(k)
+    ref_lab, ref_d = lab.clone(), d.clone()
+    assign(k)
+    same_assign = bool(torch.equal(lab, ref_lab) and torch.equal(d, ref_d))
+    t_seq = float(np.mean(cuda_time_ms(torch, lambda: assign_seq(k), 2, flush)))
+    t_asg = float(np.mean(cuda_time_ms(torch, lambda: assign(m), steps, flush)))
     return {"ms": ms, "value": m * n * T / (ms * 1e-3), "unit": "pairs/s",
+            "assign": {"ubis": m, "tol": 0.05, "ms": t_asg, "value": m * n / (t_asg * 1e-3),
+                       "sequential_plain_fp64_value": k * n / (t_seq * 1e-3),
+                       "sequential_ubis": k, "identical_to_sequential": same_assign},
             "build_ms_wall": build_ms, "cells": grid.nx ** 3, "cell_A^-1": grid.cs,
             "pairs_tested_fp64": st["pairs_tested"],
             "tested_fraction": st["pairs_tested"] / float(m * n),
@@ -537,6 +566,11 @@ def run_ours(args, rank, world, local_rank):
     refine = refine_csr_measure(torch, dev, steps=max(3, args.steps), flush=flush,
                                 cpu=(world == 1))
     adj = adjoint_measure(torch, dev, steps=max(3, args.steps))
+    # the same scoring through the reciprocal-space cell index (exact FP64 lookups)
+    cell = grid_measure(torch, dev, ps, ubis, steps=max(3, args.steps), flush=flush,
+                        check_counts=counts)
+    cell["ratio_vs_fp32_screening"] = cell["value"] / value
+    cell["ratio_vs_plain_fp64_all_tols"] = cell["value"] / rate64f
 
     # end to end through the public API: pinned host inputs -> counts on host
     gv_h = torch.tensor(ps.gv).pin_memory()
@@ -583,6 +617,7 @@ def run_ours(args, rank, world, local_rank):
         "plain_fp64": {"value_per_tol_launch": rate64, "value_all_tols": rate64f,
                        "unit": "pairs/s", "ubis": m64,
                        "ratio_vs_per_tol": value / rate64, "ratio_vs_all_tols": value / rate64f},
+        "cell_index": cell,
         "refine_csr": refine,
         "adjoint": adj,
         "compute_gv": {"peaks": 10_000_000, "ms": gv_ms, "achieved_gbs": gv_gbs,

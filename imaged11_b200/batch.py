@@ -189,6 +189,59 @@ def score_grid(ubis, grid, tols, sums=False, workspace=None, out=None):
     return (counts, s) if sums else counts
 
 
+def score_and_assign_grid(ubis, grid, tol, drlv2, labels, grain_labels=None, npk=False):
+    """score_and_assign (ImageD11 src/closest.c:366-397) for every grain in
+    order, as ImageD11/indexing.py fight_over_peaks calls it, in one pass
+    over the cell index: drlv2 (n float64) and labels (n int32) -- CUDA
+    tensors, or numpy arrays copied back in place -- end up exactly as after
+    the sequential calls score_and_assign(ubis[i], gv, tol, drlv2, labels,
+    grain_labels[i]).  grain_labels: strictly increasing ints (default
+    0 .. m-1).  With npk=True also returns the int32 count of peaks holding
+    each grain's label at the end."""
+    torch = _torch()
+    u = _dev(ubis, torch.float64).reshape(-1, 9)
+    m = u.shape[0]
+    dev = u.device
+    host = isinstance(drlv2, np.ndarray)
+    if host != isinstance(labels, np.ndarray):
+        raise TypeError("drlv2 and labels: both numpy or both CUDA tensors")
+    if host:
+        if drlv2.dtype != np.float64 or labels.dtype != np.int32:
+            raise TypeError("drlv2 must be float64 and labels int32")
+        d = torch.as_tensor(drlv2).to(dev)
+        lab = torch.as_tensor(labels).to(dev)
+    else:
+        if drlv2.dtype != torch.float64 or labels.dtype != torch.int32:
+            raise TypeError("drlv2 must be float64 and labels int32")
+        d, lab = drlv2, labels
+    if d.numel() != grid.n or lab.numel() != grid.n or not (d.is_contiguous() and
+                                                           lab.is_contiguous()):
+        raise ValueError("drlv2 and labels need one contiguous entry per g-vector")
+    gl = None
+    if grain_labels is not None:
+        gl = torch.as_tensor(np.asarray(grain_labels, dtype=np.int32)).to(dev) \
+            if not torch.is_tensor(grain_labels) else grain_labels.to(dev, torch.int32)
+        if gl.numel() != m:
+            raise ValueError("one grain label per UBI")
+        if m > 1 and not bool((gl[1:] > gl[:-1]).all()):
+            raise ValueError("grain_labels must be strictly increasing")
+        gl = gl.contiguous()
+    counts = torch.empty(m, dtype=torch.int32, device=dev) if npk else None
+    ws = torch.empty(lib.id11b_assign_workspace_bytes(grid.n), dtype=torch.uint8, device=dev)
+    check(lib.id11b_dev_score_and_assign_grid(u.data_ptr(), m,
+                                              gl.data_ptr() if gl is not None else None,
+                                              grid.gv.data_ptr(), grid.n, grid.nx,
+                                              grid.buf.data_ptr(), float(tol), d.data_ptr(),
+                                              lab.data_ptr(),
+                                              counts.data_ptr() if npk else None,
+                                              ws.data_ptr(), ws.numel(), _stream()),
+          "score_and_assign_grid")
+    if host:
+        drlv2[:] = d.cpu().numpy()
+        labels[:] = lab.cpu().numpy()
+    return counts
+
+
 def score_many_fp64(ubis, gv, tols, out=None):
     """Plain FP64 batched score (reference arithmetic).  gv: (n,3) float64 CUDA
     tensor or GvecSet.  Returns int32 (m, len(tols))."""

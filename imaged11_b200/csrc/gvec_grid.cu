@@ -23,6 +23,7 @@
 // scored by a plain scan of every regular g; g-vectors outside the regular
 // range (non-finite or |g_j| > 1024) by a scan over that list.
 #include <math.h>
+#include <limits.h>
 #include <stdint.h>
 
 #include "common.cuh"
@@ -398,13 +399,13 @@ struct Batch {
 // The lookups of `take` queued hkl (slot = lane), warp-cooperatively: the
 // cell rows of all of them are flattened across the lanes, then the g of
 // each 32 rows, so the lanes stay converged whatever the per-query sizes.
-template <int NT>
+// Every g inside a box is evaluated in the reference's FP64 arithmetic and
+// handed to act(pos, drlv2, own), own = (rounded h == the box's hkl).
+template <class Act>
 __device__ __forceinline__ void lookup_batch(const volatile WarpPlan* wp, Batch* bt,
                                              const unsigned long long* q_w, int take, int lane,
                                              const Header& H, const int* __restrict__ start,
-                                             const double* __restrict__ gs, const double* t2,
-                                             int* cnt, double* sum,
-                                             unsigned long long& tested) {
+                                             const double* __restrict__ gs, Act& act) {
     int nrows = 0;
     if (lane < take) {
         const unsigned long long q = q_w[lane];
@@ -458,16 +459,8 @@ __device__ __forceinline__ void lookup_batch(const volatile WarpPlan* wp, Batch*
 #pragma unroll
                     for (int e = 0; e < 9; e++) u[e] = wp->u[e];
                     const double sv = drlv2_exact(u, g0, g1, g2, ih);
-                    tested++;
                     unpack_hkl(bt->hkl[qq], hkl);
-                    if (ih[0] == hkl[0] && ih[1] == hkl[1] && ih[2] == hkl[2]) {
-#pragma unroll
-                        for (int j = 0; j < NT; j++)
-                            if (sv < t2[j]) {
-                                cnt[j]++;
-                                sum[j] += sv;
-                            }
-                    }
+                    act(pos, sv, ih[0] == hkl[0] && ih[1] == hkl[1] && ih[2] == hkl[2]);
                 }
             }
         }
@@ -475,19 +468,134 @@ __device__ __forceinline__ void lookup_batch(const volatile WarpPlan* wp, Batch*
     __syncwarp();
 }
 
+// Plan of UBI i into the warp's shared slot; false: plain scan instead.
+__device__ __forceinline__ bool setup_plan(volatile WarpPlan* wp, const double* __restrict__ ubis,
+                                           int64_t i, double tmax, const Header& H,
+                                           int64_t nreg, int lane) {
+    double u[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
+    const Plan P = make_plan(u, tmax, H, nreg);
+    const bool ok = P.ok && P.nh[0] < (1 << 20) && P.nh[1] < (1 << 20) && P.nh[2] < (1 << 20);
+    if (lane == 0) {
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            wp->u[e] = u[e];
+            wp->ub[e] = P.ub[e];
+        }
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            wp->w[r] = P.w[r];
+            wp->lo[r] = ok ? (int)P.lo[r] : 0;
+            wp->nh[r] = ok ? (int)P.nh[r] : 0;
+        }
+    }
+    __syncwarp();
+    return ok;
+}
+
+// Every (UBI, g) pair of work item `part` of `parts` whose drlv2 can be below
+// the plan's tolerance goes to act(pos, drlv2, own): through the hkl lookup
+// when ok, else by a plain scan of the regular g (own = true: each g once).
+template <class Act>
+__device__ __forceinline__ void walk(volatile WarpPlan* wp, Batch* bt, unsigned long long* q_w,
+                                     bool ok, int part, int parts, int lane, const Header& H,
+                                     int64_t nreg, const int* __restrict__ start,
+                                     const double* __restrict__ gs, Act& act) {
+    if (!ok) {
+        double u[9];
+#pragma unroll
+        for (int e = 0; e < 9; e++) u[e] = wp->u[e];
+        for (int64_t f = (int64_t)part * 32 + lane; f < nreg; f += 32 * (int64_t)parts) {
+            double ih[3];
+            const double s = drlv2_exact(u, gs[3 * f], gs[3 * f + 1], gs[3 * f + 2], ih);
+            act((int)f, s, true);
+        }
+        return;
+    }
+    int qn = 0;  // queued (uniform)
+    const unsigned lt = (1u << lane) - 1u;
+    const int nh0 = wp->nh[0];
+    const int64_t nhk = (int64_t)nh0 * wp->nh[1];
+    for (int64_t hb = (int64_t)part * 32; hb < nhk; hb += 32 * (int64_t)parts) {
+        const int64_t hk = hb + lane;
+        int len = 0, l0 = 0, h = 0, k = 0;
+        if (hk < nhk) {
+            h = wp->lo[0] + (int)(hk % nh0);
+            k = wp->lo[1] + (int)(hk / nh0);
+            const double bx = wp->ub[2], by = wp->ub[5], bz = wp->ub[8];  // l direction
+            const double bb = bx * bx + by * by + bz * bz;
+            const double R = (H.rmax + sqrt(wp->w[0] * wp->w[0] + wp->w[1] * wp->w[1] +
+                                            wp->w[2] * wp->w[2])) * (1. + 1e-9) + 1e-12;
+            const double ax = wp->ub[0] * h + wp->ub[1] * k, ay = wp->ub[3] * h + wp->ub[4] * k,
+                         az = wp->ub[6] * h + wp->ub[7] * k;
+            const double ab = ax * bx + ay * by + az * bz;
+            const double aa = ax * ax + ay * ay + az * az;
+            const double disc = ab * ab - bb * (aa - R * R);
+            if (disc >= 0.) {
+                const double sq = sqrt(disc);
+                const double la = fmax(floor((-ab - sq) / bb) - 1., (double)wp->lo[2]);
+                const double lb = fmin(ceil((-ab + sq) / bb) + 1.,
+                                       (double)(wp->lo[2] + wp->nh[2] - 1));
+                if (la <= lb) {
+                    l0 = (int)la;
+                    len = (int)(lb - la) + 1;
+                }
+            }
+        }
+        int total;
+        const int excl = warp_excl_scan(len, lane, total);
+        for (int f0 = 0; f0 < total; f0 += 32) {
+            const int f = f0 + lane;
+            const int j = owner(excl, f);
+            const int hj = __shfl_sync(0xffffffffu, h, j);
+            const int kj = __shfl_sync(0xffffffffu, k, j);
+            const int lj = __shfl_sync(0xffffffffu, l0, j) + f - __shfl_sync(0xffffffffu, excl, j);
+            bool pass = false;
+            if (f < total) {
+                const double hkl[3] = {(double)hj, (double)kj, (double)lj};
+                bool in = true;
+                double d2 = 0.;
+                const double G = -H.lo;
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    const double c = wp->ub[3 * r] * hkl[0] + wp->ub[3 * r + 1] * hkl[1] +
+                                     wp->ub[3 * r + 2] * hkl[2];
+                    const double wr = wp->w[r];
+                    in = in && (c - wr <= G) && (c + wr >= -G);
+                    const double e = fmax(fabs(c) - wr, 0.);
+                    d2 += e * e;
+                }
+                pass = in && d2 <= H.rmax * H.rmax * (1. + 1e-9);
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, pass);
+            if (pass) q_w[qn + __popc(mask & lt)] = pack_hkl(hj, kj, lj);
+            qn += __popc(mask);
+            __syncwarp();
+            if (qn >= 32) {
+                lookup_batch(wp, bt, q_w, 32, lane, H, start, gs, act);
+                const int rest = qn - 32;
+                unsigned long long v = 0;
+                if (lane < rest) v = q_w[32 + lane];
+                __syncwarp();
+                if (lane < rest) q_w[lane] = v;
+                __syncwarp();
+                qn = rest;
+            }
+        }
+    }
+    if (qn > 0) lookup_batch(wp, bt, q_w, qn, lane, H, start, gs, act);
+}
+
 template <int NT>
 __global__ void __launch_bounds__(kST, ID11B_GRID_MINB)
 k_score(const double* __restrict__ ubis, int64_t m, int parts, Header* __restrict__ Hp,
-        const int* __restrict__ start, const double* __restrict__ gs,
-        Tols tols, int* __restrict__ pcnt,
-        double* __restrict__ psum) {
+        const int* __restrict__ start, const double* __restrict__ gs, Tols tols,
+        int* __restrict__ pcnt, double* __restrict__ psum) {
     __shared__ unsigned long long s_q[kSW][kQueue];
     __shared__ WarpPlan s_plan[kSW];
     __shared__ Batch s_batch[kSW];
-    Batch* bt = s_batch + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    unsigned long long* q_w = s_q[threadIdx.x >> 5];
-    volatile WarpPlan* wp = s_plan + (threadIdx.x >> 5);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t wk = ((int64_t)blockIdx.x * kST + threadIdx.x) >> 5;
     if (wk >= m * parts) return;  // uniform per warp
     const int64_t i = wk / parts;
@@ -496,49 +604,20 @@ k_score(const double* __restrict__ ubis, int64_t m, int parts, Header* __restric
     const int64_t nreg = start[H.ncells];
     double t2[NT];
     double tmax = 0.;
-#pragma unroll
-    for (int j = 0; j < NT; j++) {
-        tmax = fmax(tmax, tols.t[j]);
-        t2[j] = tols.t[j] * tols.t[j];
-    }
     int cnt[NT];
     double sum[NT];
 #pragma unroll
     for (int j = 0; j < NT; j++) {
+        tmax = fmax(tmax, tols.t[j]);
+        t2[j] = tols.t[j] * tols.t[j];
         cnt[j] = 0;
         sum[j] = 0.;
     }
     unsigned long long tested = 0;
-    bool ok;
-    {
-        double u[9];
-#pragma unroll
-        for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
-        const Plan P = make_plan(u, tmax, H, nreg);
-        ok = P.ok && P.nh[0] < (1 << 20) && P.nh[1] < (1 << 20) && P.nh[2] < (1 << 20);
-        if (lane == 0) {
-#pragma unroll
-            for (int e = 0; e < 9; e++) {
-                wp->u[e] = u[e];
-                wp->ub[e] = P.ub[e];
-            }
-#pragma unroll
-            for (int r = 0; r < 3; r++) {
-                wp->w[r] = P.w[r];
-                wp->lo[r] = ok ? (int)P.lo[r] : 0;
-                wp->nh[r] = ok ? (int)P.nh[r] : 0;
-            }
-        }
-        __syncwarp();
-    }
-    if (!ok) {
-        double u[9];
-#pragma unroll
-        for (int e = 0; e < 9; e++) u[e] = wp->u[e];
-        for (int64_t f = (int64_t)part * 32 + lane; f < nreg; f += 32 * (int64_t)parts) {
-            double ih[3];
-            const double s = drlv2_exact(u, gs[3 * f], gs[3 * f + 1], gs[3 * f + 2], ih);
-            tested++;
+    const bool ok = setup_plan(s_plan + w, ubis, i, tmax, H, nreg, lane);
+    auto act = [&](int, double s, bool own) {
+        tested++;
+        if (own) {
 #pragma unroll
             for (int j = 0; j < NT; j++)
                 if (s < t2[j]) {
@@ -546,95 +625,9 @@ k_score(const double* __restrict__ ubis, int64_t m, int parts, Header* __restric
                     sum[j] += s;
                 }
         }
-        if (part == 0 && lane == 0) atomicAdd(&Hp->nfallback, 1ull);
-    } else {
-        int qn = 0;  // queued (uniform)
-        const unsigned lt = (1u << lane) - 1u;
-        const int nh0 = wp->nh[0];
-        const int64_t nhk = (int64_t)nh0 * wp->nh[1];
-        for (int64_t hb = (int64_t)part * 32; hb < nhk; hb += 32 * (int64_t)parts) {
-            const int64_t hk = hb + lane;
-            int len = 0, l0 = 0, h = 0, k = 0;
-            if (hk < nhk) {
-                h = wp->lo[0] + (int)(hk % nh0);
-                k = wp->lo[1] + (int)(hk / nh0);
-                const double bx = wp->ub[2], by = wp->ub[5], bz = wp->ub[8];  // l direction
-                const double bb = bx * bx + by * by + bz * bz;
-                const double R = (H.rmax + sqrt(wp->w[0] * wp->w[0] + wp->w[1] * wp->w[1] +
-                                                wp->w[2] * wp->w[2])) * (1. + 1e-9) + 1e-12;
-                const double ax = wp->ub[0] * h + wp->ub[1] * k,
-                             ay = wp->ub[3] * h + wp->ub[4] * k,
-                             az = wp->ub[6] * h + wp->ub[7] * k;
-                const double ab = ax * bx + ay * by + az * bz;
-                const double aa = ax * ax + ay * ay + az * az;
-                const double disc = ab * ab - bb * (aa - R * R);
-                if (disc >= 0.) {
-                    const double sq = sqrt(disc);
-                    const double la = fmax(floor((-ab - sq) / bb) - 1., (double)wp->lo[2]);
-                    const double lb = fmin(ceil((-ab + sq) / bb) + 1.,
-                                           (double)(wp->lo[2] + wp->nh[2] - 1));
-                    if (la <= lb) {
-                        l0 = (int)la;
-                        len = (int)(lb - la) + 1;
-                    }
-                }
-            }
-            int incl = len;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            const int excl = incl - len;
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            for (int f0 = 0; f0 < total; f0 += 32) {
-                const int f = f0 + lane;
-                int j = 0;  // largest lane j with excl_j <= f
-#pragma unroll
-                for (int st = 16; st > 0; st >>= 1) {
-                    const int v = __shfl_sync(0xffffffffu, excl, j + st);
-                    if (v <= f) j += st;
-                }
-                const int hj = __shfl_sync(0xffffffffu, h, j);
-                const int kj = __shfl_sync(0xffffffffu, k, j);
-                const int lj = __shfl_sync(0xffffffffu, l0, j) + f -
-                               __shfl_sync(0xffffffffu, excl, j);
-                bool pass = false;
-                if (f < total) {
-                    const double hkl[3] = {(double)hj, (double)kj, (double)lj};
-                    double c[3];
-                    bool in = true;
-                    double d2 = 0.;
-                    const double G = -H.lo;
-#pragma unroll
-                    for (int r = 0; r < 3; r++) {
-                        c[r] = wp->ub[3 * r] * hkl[0] + wp->ub[3 * r + 1] * hkl[1] +
-                               wp->ub[3 * r + 2] * hkl[2];
-                        const double wr = wp->w[r];
-                        in = in && (c[r] - wr <= G) && (c[r] + wr >= -G);
-                        const double e = fmax(fabs(c[r]) - wr, 0.);
-                        d2 += e * e;
-                    }
-                    pass = in && d2 <= H.rmax * H.rmax * (1. + 1e-9);
-                }
-                const unsigned mask = __ballot_sync(0xffffffffu, pass);
-                if (pass) q_w[qn + __popc(mask & lt)] = pack_hkl(hj, kj, lj);
-                qn += __popc(mask);
-                __syncwarp();
-                if (qn >= 32) {
-                    lookup_batch<NT>(wp, bt, q_w, 32, lane, H, start, gs, t2, cnt, sum, tested);
-                    const int rest = qn - 32;
-                    unsigned long long v = 0;
-                    if (lane < rest) v = q_w[32 + lane];
-                    __syncwarp();
-                    if (lane < rest) q_w[lane] = v;
-                    __syncwarp();
-                    qn = rest;
-                }
-            }
-        }
-        if (qn > 0) lookup_batch<NT>(wp, bt, q_w, qn, lane, H, start, gs, t2, cnt, sum, tested);
-    }
+    };
+    walk(s_plan + w, s_batch + w, s_q[w], ok, part, parts, lane, H, nreg, start, gs, act);
+    if (!ok && part == 0 && lane == 0) atomicAdd(&Hp->nfallback, 1ull);
 #pragma unroll
     for (int j = 0; j < NT; j++) {
         const int cs = warp_sum(cnt[j]);
@@ -683,6 +676,122 @@ k_score_finish(const double* __restrict__ ubis, int64_t m, int parts, int ntol, 
     for (int j = 0; j < ntol; j++) {
         counts[i * ntol + j] = c[j];
         if (sums) sums[i * ntol + j] = s[j];
+    }
+}
+
+// ------------------------------------------------------------ assignment --
+// Batched score_and_assign (ImageD11 src/closest.c:366-397) over m grains in
+// order: for each g the reference's sequence of calls leaves the label of the
+// first grain reaching the smallest drlv2 among those below tol^2 and below
+// the g's initial drlv2, and that drlv2.  Pass 0 takes the minimum (FP64 bits
+// of non-negative values order like the values), pass 1 the lowest grain index
+// reaching it; both passes evaluate the same pairs with the same arithmetic.
+template <int PASS>
+__global__ void __launch_bounds__(kST, ID11B_GRID_MINB)
+k_assign(const double* __restrict__ ubis, int64_t m, int parts, const Header* __restrict__ Hp,
+         const int* __restrict__ start, const double* __restrict__ gs,
+         const int* __restrict__ gidx, double tol, const double* __restrict__ drlv2,
+         unsigned long long* __restrict__ best, int* __restrict__ lab) {
+    __shared__ unsigned long long s_q[kSW][kQueue];
+    __shared__ WarpPlan s_plan[kSW];
+    __shared__ Batch s_batch[kSW];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t wk = ((int64_t)blockIdx.x * kST + threadIdx.x) >> 5;
+    if (wk >= m * parts) return;  // uniform per warp
+    const int64_t i = wk / parts;
+    const int part = (int)(wk % parts);
+    const Header H = *Hp;
+    const int64_t nreg = start[H.ncells];
+    const double t2 = tol * tol;
+    const bool ok = setup_plan(s_plan + w, ubis, i, tol, H, nreg, lane);
+    auto act = [&](int pos, double s, bool own) {
+        if (!own || !(s < t2)) return;
+        const int k = __ldg(gidx + pos);
+        if (!(s < __ldg(drlv2 + k))) return;
+        const unsigned long long b = (unsigned long long)__double_as_longlong(s);
+        if (PASS == 0)
+            atomicMin(best + k, b);
+        else if (best[k] == b)
+            atomicMin(lab + k, (int)i);
+    };
+    walk(s_plan + w, s_batch + w, s_q[w], ok, part, parts, lane, H, nreg, start, gs, act);
+}
+
+__global__ void __launch_bounds__(kGT)
+k_assign_init(int64_t n, unsigned long long* __restrict__ best, int* __restrict__ lab) {
+    for (int64_t k = (int64_t)blockIdx.x * kGT + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * kGT) {
+        best[k] = ~0ull;
+        lab[k] = INT_MAX;
+    }
+}
+
+// is v one of the grain labels (strictly increasing; null: 0 .. m-1)?
+__device__ __forceinline__ bool is_grain_label(int v, const int* __restrict__ gl, int64_t m) {
+    if (!gl) return v >= 0 && (int64_t)v < m;
+    int64_t lo = 0, hi = m;  // binary search
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        const int x = gl[mid];
+        if (x == v) return true;
+        if (x < v) lo = mid + 1; else hi = mid;
+    }
+    return false;
+}
+
+// regular g (by sorted position): write the winner, or apply the reference's
+// "it does not belong after all" reset when the g held a grain's label
+__global__ void __launch_bounds__(kGT)
+k_assign_final(const int* __restrict__ start, int64_t ncells, const int* __restrict__ gidx,
+               const unsigned long long* __restrict__ best, const int* __restrict__ lab,
+               const int* __restrict__ gl, int64_t m, double* __restrict__ drlv2,
+               int* __restrict__ labels, int* __restrict__ npk) {
+    const int64_t nreg = start[ncells];
+    for (int64_t p = (int64_t)blockIdx.x * kGT + threadIdx.x; p < nreg;
+         p += (int64_t)gridDim.x * kGT) {
+        const int k = gidx[p];
+        const int w = lab[k];
+        if (w != INT_MAX) {
+            labels[k] = gl ? gl[w] : w;
+            drlv2[k] = __longlong_as_double((long long)best[k]);
+            if (npk) atomicAdd(npk + w, 1);
+        } else if (is_grain_label(labels[k], gl, m)) {
+            labels[k] = -1;
+        }
+    }
+}
+
+// g outside the regular range: the reference's sequence of calls, literally
+__global__ void __launch_bounds__(kGT)
+k_assign_special(const double* __restrict__ ubis, int64_t m, const double* __restrict__ gv,
+                 const int* __restrict__ spec, const int* __restrict__ nspec, double tol,
+                 const int* __restrict__ gl, double* __restrict__ drlv2,
+                 int* __restrict__ labels, int* __restrict__ npk) {
+    const int ns = *nspec;
+    const double t2 = tol * tol;
+    for (int q = blockIdx.x * kGT + threadIdx.x; q < ns; q += gridDim.x * kGT) {
+        const int64_t k = spec[q];
+        const double g0 = gv[3 * k], g1 = gv[3 * k + 1], g2 = gv[3 * k + 2];
+        double d = drlv2[k];
+        int l = labels[k];
+        int64_t win = -1;
+        for (int64_t i = 0; i < m; i++) {
+            double u[9], ih[3];
+            for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
+            const double s = drlv2_exact(u, g0, g1, g2, ih);
+            const int li = gl ? gl[i] : (int)i;
+            if (s < t2 && s < d) {
+                l = li;
+                d = s;
+                win = i;
+            } else if (l == li) {
+                l = -1;
+                win = -1;
+            }
+        }
+        labels[k] = l;
+        drlv2[k] = d;
+        if (npk && win >= 0) atomicAdd(npk + win, 1);
     }
 }
 
@@ -881,5 +990,53 @@ extern "C" int id11b_grid_stats(const void* gridbuf, int64_t* nregular, int64_t*
     if (nspecial) *nspecial = ns;
     if (nfallback) *nfallback = (int64_t)h.nfallback;
     if (ntested) *ntested = (int64_t)h.ntested;
+    return ID11B_OK;
+}
+
+extern "C" int64_t id11b_assign_workspace_bytes(int64_t n) {
+    if (n < 0) return -1;
+    const size_t nn = (size_t)(n > 0 ? n : 1);
+    return (int64_t)(al256(sizeof(unsigned long long) * nn) + al256(sizeof(int) * nn));
+}
+
+extern "C" int id11b_dev_score_and_assign_grid(const double* ubis, int64_t m,
+                                               const int32_t* grain_labels, const double* gv,
+                                               int64_t n, int32_t nx, const void* gridbuf,
+                                               double tol, double* drlv2, int32_t* labels,
+                                               int32_t* npk, void* ws, int64_t ws_bytes,
+                                               void* stream) {
+    if (m < 0 || n < 0 || nx < 1 || nx > 400 || !gridbuf || !ws || (m > 0 && !ubis) ||
+        (n > 0 && (!gv || !drlv2 || !labels)) || !(tol >= 0.) || !(tol < 1e3))
+        return ID11B_ERR_ARG;
+    if (((uintptr_t)gridbuf & 255) || ((uintptr_t)ws & 255)) return ID11B_ERR_ALIGN;
+    if (ws_bytes < id11b_assign_workspace_bytes(n)) return ID11B_ERR_SIZE;
+    if (m > INT32_MAX - 1) return ID11B_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (npk && m > 0) ID11B_CHECK(cudaMemsetAsync(npk, 0, sizeof(int32_t) * (size_t)m, st));
+    if (m == 0 || n == 0) return ID11B_OK;
+    const int64_t ncells = (int64_t)nx * nx * nx;
+    const Layout L = layout(n, ncells);
+    const char* b = (const char*)gridbuf;
+    const Header* H = (const Header*)b;
+    const int* start = (const int*)(b + L.start);
+    const double* gs = (const double*)(b + L.g);
+    const int* gidx = (const int*)(b + L.idx);
+    unsigned long long* best = (unsigned long long*)ws;
+    int* lab = (int*)((char*)ws + al256(sizeof(unsigned long long) * (size_t)n));
+    k_assign_init<<<grid_for(n, kGT), kGT, 0, st>>>(n, best, lab);
+    ID11B_CHECK_LAUNCH();
+    const int parts = score_parts(m);
+    const unsigned blocks = (unsigned)((m * parts + kSW - 1) / kSW);
+    k_assign<0><<<blocks, kST, 0, st>>>(ubis, m, parts, H, start, gs, gidx, tol, drlv2, best, lab);
+    ID11B_CHECK_LAUNCH();
+    k_assign<1><<<blocks, kST, 0, st>>>(ubis, m, parts, H, start, gs, gidx, tol, drlv2, best, lab);
+    ID11B_CHECK_LAUNCH();
+    k_assign_final<<<grid_for(n, kGT), kGT, 0, st>>>(start, ncells, gidx, best, lab, grain_labels,
+                                                     m, drlv2, labels, npk);
+    ID11B_CHECK_LAUNCH();
+    k_assign_special<<<grid_for(n, kGT), kGT, 0, st>>>(ubis, m, gv, (const int*)(b + L.spec),
+                                                       (const int*)(b + L.spos) + n, tol,
+                                                       grain_labels, drlv2, labels, npk);
+    ID11B_CHECK_LAUNCH();
     return ID11B_OK;
 }

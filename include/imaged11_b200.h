@@ -249,6 +249,23 @@ int id11b_dev_score_grid(const double *ubis, int64_t m, const double *gv, int64_
 int id11b_grid_stats(const void *gridbuf, int64_t *nregular, int64_t *nspecial,
                      int64_t *nfallback, int64_t *ntested, void *stream);
 
+/* Batched score_and_assign through the cell index: the result of calling the
+ * reference's score_and_assign (ImageD11 src/closest.c:366-397) for grain
+ * i = 0 .. m-1 in order, score_and_assign(ubis[i], gv, tol, drlv2, labels,
+ * grain_labels[i]), as ImageD11/indexing.py fight_over_peaks (:876-905) does:
+ * drlv2 (n) and labels (n) are updated in place to the same values, bit for
+ * bit.  grain_labels: strictly increasing int32 (m), or NULL for 0 .. m-1
+ * (the caller checks the order).  npk (m, optional): peaks holding each
+ * grain's label at the end (the histogram fight_over_peaks takes); the
+ * per-call return values of the sequential calls are not reproduced.  ws:
+ * id11b_assign_workspace_bytes(n), 256-byte aligned. */
+int64_t id11b_assign_workspace_bytes(int64_t n);
+int id11b_dev_score_and_assign_grid(const double *ubis, int64_t m, const int32_t *grain_labels,
+                                    const double *gv, int64_t n, int32_t nx,
+                                    const void *gridbuf, double tol, double *drlv2,
+                                    int32_t *labels, int32_t *npk, void *ws, int64_t ws_bytes,
+                                    void *stream);
+
 /* `iters` rounds of score_and_refine (ImageD11 src/closest.c:267-345) for each
  * of m UBIs against all n g-vectors, ubis (m,3,3) updated in place; npk and
  * mean_drlv2 (optional) receive the last round's count and mean drlv2.

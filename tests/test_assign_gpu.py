@@ -1,0 +1,90 @@
+"""Batched score_and_assign through the cell index vs the oracle's sequence
+of score_and_assign calls (the loop of ImageD11/indexing.py fight_over_peaks).
+
+Labels and drlv2 must match the sequential calls bit for bit: ties go to the
+first grain, the reference's "does not belong after all" reset applies to g
+that held a grain's label, and g outside the regular range follow the same
+sequence of calls."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def sequential(oracle, ubis, gv, tol, drlv2, labels, grain_labels):
+    d, lab = drlv2.copy(), labels.copy()
+    for u, gl in zip(ubis, grain_labels):
+        _, d, lab = oracle.score_and_assign(u, gv, tol, d, lab, int(gl))
+    return d, lab
+
+
+@pytest.fixture(scope="module")
+def scene():
+    from imaged11_b200 import synth
+    ps = synth.simulate(150, "Al", gmax=1.3, seed=61, noise_frac=0.10)
+    rng = np.random.default_rng(62)
+    ubis = synth.trial_ubis(ps.ubis, 400, 0.5, 0.3, rng)
+    return ps, ubis
+
+
+@pytest.mark.parametrize("tol", [0.02, 0.1, 0.3])
+def test_fight_over_peaks(scene, oracle, tol, cuda):
+    from imaged11_b200 import batch
+    ps, ubis = scene
+    n = len(ps.gv)
+    d0 = np.zeros(n) + 2
+    l0 = np.zeros(n, np.int32) - 1
+    ref_d, ref_l = sequential(oracle, ubis, ps.gv, tol, d0, l0, range(len(ubis)))
+    d, lab = d0.copy(), l0.copy()
+    npk = batch.score_and_assign_grid(ubis, batch.GvecGrid(ps.gv), tol, d, lab, npk=True)
+    assert np.array_equal(lab, ref_l)
+    assert np.array_equal(d, ref_d)
+    hist = np.bincount(ref_l[ref_l >= 0], minlength=len(ubis))
+    assert np.array_equal(npk.cpu().numpy(), hist)
+
+
+def test_ties_labels_and_resets(scene, oracle, cuda):
+    from imaged11_b200 import batch
+    ps, ubis = scene
+    u = ubis[:60].copy()
+    u[7] = u[3]                       # exact ties: the first grain keeps the peak
+    u[11] = 0.0                       # singular: plain scan
+    u[13, 0, 0] = np.nan
+    gl = np.arange(60, dtype=np.int32) * 10 + 5
+    n = len(ps.gv)
+    rng = np.random.default_rng(63)
+    d0 = rng.uniform(0.0, 0.02, n)    # some peaks already well assigned
+    d0[rng.random(n) < 0.05] = -1.0   # never reassigned
+    l0 = rng.choice(np.concatenate([gl, [-1, 3, 99999]]), n).astype(np.int32)
+    ref_d, ref_l = sequential(oracle, u, ps.gv, 0.08, d0, l0, gl)
+    d, lab = d0.copy(), l0.copy()
+    batch.score_and_assign_grid(u, batch.GvecGrid(ps.gv), 0.08, d, lab, grain_labels=gl)
+    assert np.array_equal(lab, ref_l)
+    assert np.array_equal(d, ref_d)
+
+
+def test_special_g_and_device_tensors(golden, oracle, cuda):
+    import torch
+    from imaged11_b200 import batch
+    dd = golden["scoring"]
+    gv = dd["adv_gv"]
+    ubis = np.concatenate([dd["adv_ubi"][None], dd["sc_ubis"][:9]])
+    n = len(gv)
+    d0 = np.zeros(n) + 2
+    l0 = np.zeros(n, np.int32) - 1
+    ref_d, ref_l = sequential(oracle, ubis, gv, 0.1, d0, l0, range(len(ubis)))
+    d = torch.tensor(d0, device="cuda")
+    lab = torch.tensor(l0, device="cuda")
+    batch.score_and_assign_grid(ubis, batch.GvecGrid(gv), 0.1, d, lab)
+    assert np.array_equal(lab.cpu().numpy(), ref_l)
+    assert np.array_equal(d.cpu().numpy(), ref_d, equal_nan=True)
+
+
+def test_bad_grain_labels(scene, cuda):
+    from imaged11_b200 import batch
+    ps, ubis = scene
+    n = len(ps.gv)
+    d, lab = np.zeros(n) + 2, np.zeros(n, np.int32) - 1
+    with pytest.raises(ValueError):
+        batch.score_and_assign_grid(ubis[:3], batch.GvecGrid(ps.gv), 0.1, d, lab,
+                                    grain_labels=[3, 2, 5])

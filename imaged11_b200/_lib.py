@@ -36,6 +36,8 @@ _SIGNATURES = [
     ("id11b_dev_compute_gv", _i, [_p, _p, _d, _d, _d, _d, _p, _p, _p, _i64, _p]),
     ("id11b_dev_compute_geometry", _i, [_p, _p, _d, _d, _d, _d, _p, _p, _i64, _p]),
     ("id11b_dev_compute_xlylzl", _i, [_p, _p, _p, _p, _p, _p, _i64, _p]),
+    ("id11b_dev_update_geometry", _i, [_p, _p, _p, _p, _p, _p, _d, _d, _d, _d, _p, _p, _p, _p,
+                                        _i64, _p]),
     ("id11b_dev_score", _i, [_p, _p, _d, _i64, _p, _p]),
     ("id11b_lsq_workspace_bytes", _i64, [_i64]),
     ("id11b_dev_score_and_refine", _i, [_p, _p, _d, _i64, _p, _p, _p, _i64, _p]),

@@ -84,6 +84,16 @@ __device__ __forceinline__ void peak_geometry(const GvParams& P, double x0, doub
     r.g2 = v2;
 }
 
+// tth, eta, ds, g of one peak (ImageD11 src/cdiffraction.c:74-91)
+__device__ __forceinline__ void geometry_out(const PeakGeo& r, double* o) {
+    o[0] = dmul(kDeg, atan2(__dsqrt_rn(dadd(dmul(r.d1, r.d1), dmul(r.d2, r.d2))), r.d0));
+    o[1] = dmul(kDeg, atan2(-r.d1, r.d2));
+    o[2] = __dsqrt_rn(ddot3(r.k0, r.k1, r.k2, r.k0, r.k1, r.k2));
+    o[3] = r.g0;
+    o[4] = r.g1;
+    o[5] = r.g2;
+}
+
 // MODE 0: gv (n,3); MODE 1: geometry out (n,6)
 template <int MODE>
 __global__ void __launch_bounds__(kGeoThreads)
@@ -114,15 +124,7 @@ k_geometry(const double* __restrict__ xyz, const double* __restrict__ omega, GvP
                 if (g4)
                     g4[base + tid] = make_float4((float)r.g0, (float)r.g1, (float)r.g2, 0.f);
             } else {
-                // ImageD11 src/cdiffraction.c:74-91
-                double* o = s_out + 6 * tid;
-                o[0] = dmul(kDeg, atan2(__dsqrt_rn(dadd(dmul(r.d1, r.d1), dmul(r.d2, r.d2))),
-                                        r.d0));
-                o[1] = dmul(kDeg, atan2(-r.d1, r.d2));
-                o[2] = __dsqrt_rn(ddot3(r.k0, r.k1, r.k2, r.k0, r.k1, r.k2));
-                o[3] = r.g0;
-                o[4] = r.g1;
-                o[5] = r.g2;
+                geometry_out(r, s_out + 6 * tid);
             }
         }
         __syncthreads();
@@ -211,14 +213,7 @@ k_geometry_tma(const double* __restrict__ xyz, const double* __restrict__ omega,
                 s_out[3 * tid + 2] = r.g2;
                 if (g4) g4[base + tid] = make_float4((float)r.g0, (float)r.g1, (float)r.g2, 0.f);
             } else {
-                double* o = s_out + 6 * tid;
-                o[0] = dmul(kDeg, atan2(__dsqrt_rn(dadd(dmul(r.d1, r.d1), dmul(r.d2, r.d2))),
-                                        r.d0));
-                o[1] = dmul(kDeg, atan2(-r.d1, r.d2));
-                o[2] = __dsqrt_rn(ddot3(r.k0, r.k1, r.k2, r.k0, r.k1, r.k2));
-                o[3] = r.g0;
-                o[4] = r.g1;
-                o[5] = r.g2;
+                geometry_out(r, s_out + 6 * tid);
             }
         }
         __syncthreads();  // stage consumed by every lane; s_out complete
@@ -268,6 +263,71 @@ k_xlylzl(const double* __restrict__ s, const double* __restrict__ f, XyzParams P
         for (int j = 0; j < 3; j++) {
             int e = tid + j * kGeoThreads;
             if (e < 3 * cnt) __stcs(dst + e, s_out[e]);
+        }
+        __syncthreads();
+    }
+}
+
+// Detector position -> lab position -> geometry in one pass (the two calls of
+// columnfile.updateGeometry's fast path, ImageD11/columnfile.py:497-504:
+// Ctransform.sf2xyz = compute_xlylzl, then xyz2geometry = compute_geometry).
+// The lab positions never leave registers unless asked for, and each value is
+// produced by the same operations as the two separate kernels, so the results
+// are identical to calling them in turn.  sc, fc, omega are read once with
+// the next tile's loads issued before the current tile is computed.
+template <bool XYZ, bool G4>
+__global__ void __launch_bounds__(kGeoThreads, 4)
+k_update_geometry(const double* __restrict__ sc, const double* __restrict__ fc,
+                  const double* __restrict__ omega, XyzParams X, GvParams P,
+                  double* __restrict__ xyz, double* __restrict__ out, float4* __restrict__ g4,
+                  int64_t n) {
+    __shared__ double s_xyz[XYZ ? 3 * kGeoThreads : 1];
+    __shared__ double s_out[6 * kGeoThreads];
+    const int tid = threadIdx.x;
+    const int64_t ntiles = (n + kGeoThreads - 1) / kGeoThreads;
+    double sn = 0., fn = 0., on = 0.;
+    auto load = [&](int64_t t) {
+        const int64_t k = t * kGeoThreads + tid;
+        if (t < ntiles && k < n) {
+            sn = __ldcs(sc + k);
+            fn = __ldcs(fc + k);
+            on = __ldcs(omega + k);
+        }
+    };
+    load(blockIdx.x);
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const double s = sn, f = fn, om = on;
+        load(t + gridDim.x);
+        const int64_t base = t * kGeoThreads;
+        const int cnt = (int)min((int64_t)kGeoThreads, n - base);
+        if (tid < cnt) {
+            const double v1 = dmul(dsub(f, X.p[1]), X.p[3]);
+            const double v2 = dmul(dsub(s, X.p[0]), X.p[2]);
+            double x[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                x[j] = dadd(dadd(dmul(X.r[3 * j + 1], v1), dmul(X.r[3 * j + 2], v2)), X.dist[j]);
+                if (XYZ) s_xyz[3 * tid + j] = x[j];
+            }
+            PeakGeo r;
+            peak_geometry(P, x[0], x[1], x[2], om, r);
+            geometry_out(r, s_out + 6 * tid);
+            if (G4) g4[base + tid] = make_float4((float)r.g0, (float)r.g1, (float)r.g2, 0.f);
+        }
+        __syncthreads();
+        if (XYZ) {
+            double* dx = xyz + 3 * base;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int e = tid + j * kGeoThreads;
+                if (e < 3 * cnt) __stcs(dx + e, s_xyz[e]);
+            }
+        }
+        double* dst = out + 6 * base;
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            const int e = tid + j * kGeoThreads;
+            if (e < 6 * cnt) __stcs(dst + e, s_out[e]);
         }
         __syncthreads();
     }
@@ -398,6 +458,39 @@ extern "C" int id11b_dev_compute_xlylzl(const double* s, const double* f,
     for (int i = 0; i < 9; i++) P.r[i] = r_host[i];
     for (int i = 0; i < 3; i++) P.dist[i] = dist_host[i];
     k_xlylzl<<<geo_grid(n), kGeoThreads, 0, (cudaStream_t)stream>>>(s, f, P, xlylzl, n);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+extern "C" int id11b_dev_update_geometry(const double* sc, const double* fc, const double* omega,
+                                         const double* p_host, const double* r_host,
+                                         const double* dist_host, double omegasign, double wvln,
+                                         double wedge, double chi, const double* t_host,
+                                         double* xlylzl, double* out, float* g4, int64_t n,
+                                         void* stream) {
+    if (n < 0 || !p_host || !r_host || !dist_host || !t_host) return ID11B_ERR_ARG;
+    if (n == 0) return ID11B_OK;
+    if (!sc || !fc || !omega || !out) return ID11B_ERR_ARG;
+    if (g4 && ((uintptr_t)g4 & 15)) return ID11B_ERR_ALIGN;
+    XyzParams X;
+    for (int i = 0; i < 4; i++) X.p[i] = p_host[i];
+    for (int i = 0; i < 9; i++) X.r[i] = r_host[i];
+    for (int i = 0; i < 3; i++) X.dist[i] = dist_host[i];
+    GvParams P = make_gv_params(omegasign, wvln, wedge, chi, t_host);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int grid = geo_grid_tma(n);
+    if (xlylzl && g4)
+        k_update_geometry<true, true><<<grid, kGeoThreads, 0, st>>>(sc, fc, omega, X, P, xlylzl,
+                                                                    out, (float4*)g4, n);
+    else if (xlylzl)
+        k_update_geometry<true, false><<<grid, kGeoThreads, 0, st>>>(sc, fc, omega, X, P, xlylzl,
+                                                                     out, nullptr, n);
+    else if (g4)
+        k_update_geometry<false, true><<<grid, kGeoThreads, 0, st>>>(sc, fc, omega, X, P, nullptr,
+                                                                     out, (float4*)g4, n);
+    else
+        k_update_geometry<false, false><<<grid, kGeoThreads, 0, st>>>(sc, fc, omega, X, P,
+                                                                      nullptr, out, nullptr, n);
     ID11B_CHECK_LAUNCH();
     return ID11B_OK;
 }

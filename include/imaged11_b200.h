@@ -179,6 +179,21 @@ int id11b_dev_score_many_fp64(const double *ubis, int64_t m, const double *gv, i
                               const double *tols_host, int ntol, int32_t *counts,
                               void *stream);
 
+/* compute_xlylzl followed by compute_geometry in one pass (the fast path of
+ * ImageD11/columnfile.py updateGeometry, :497-504: Ctransform.sf2xyz then
+ * xyz2geometry, ImageD11/transform.py:695-706, :754-774): slow/fast detector
+ * positions sc, fc and omega (n doubles each) -> out (n,6) = tth, eta, ds,
+ * gx, gy, gz, identical to the two reference calls in turn.  p, r, dist as
+ * for compute_xlylzl; omegasign, wvln, wedge, chi, t as for compute_geometry.
+ * xlylzl (n,3, optional) receives the lab positions; g4 (n float4, optional,
+ * 16-byte aligned) the FP32 g copy of id11b_dev_prepare_gvecs.  No reference
+ * counterpart as one function. */
+int id11b_dev_update_geometry(const double *sc, const double *fc, const double *omega,
+                              const double *p_host, const double *r_host,
+                              const double *dist_host, double omegasign, double wvln,
+                              double wedge, double chi, const double *t_host, double *xlylzl,
+                              double *out, float *g4, int64_t n, void *stream);
+
 /* Prepare g-vectors for the FP32 batched kernels: g4 (n float4, 16-byte
  * aligned) receives FP32 copies; gws (id11b_gvec_workspace_bytes(n), 256-byte
  * aligned) receives max|g| and the list of g evaluated in FP64 only

@@ -394,7 +394,50 @@ struct Batch {
     double c[32][3];
     unsigned long long hkl[32];
     int ix0[32], ix1[32], iy0[32], ny[32], iz0[32];
+    // g found inside a box, waiting for the FP64 evaluation (32 at a time)
+    double cg[64][3];
+    unsigned long long ch[64];
+    int cp[64];
+    int cn;
 };
+
+// Evaluate the first `take` waiting candidates (one per lane) in the
+// reference's FP64 arithmetic, hand them to act, and drop them from the list.
+template <class Act>
+__device__ __forceinline__ void eval_candidates(const volatile WarpPlan* wp, Batch* bt, int take,
+                                                int lane, Act& act) {
+    if (lane < take) {
+        double u[9], ih[3], hkl[3];
+#pragma unroll
+        for (int e = 0; e < 9; e++) u[e] = wp->u[e];
+        const double sv = drlv2_exact(u, bt->cg[lane][0], bt->cg[lane][1], bt->cg[lane][2], ih);
+        unpack_hkl(bt->ch[lane], hkl);
+        act(bt->cp[lane], sv, ih[0] == hkl[0] && ih[1] == hkl[1] && ih[2] == hkl[2]);
+    }
+    __syncwarp();
+    const int rest = bt->cn - take;  // < 32
+    double a = 0., b = 0., c = 0.;
+    unsigned long long h = 0;
+    int q = 0;
+    if (lane < rest) {
+        a = bt->cg[take + lane][0];
+        b = bt->cg[take + lane][1];
+        c = bt->cg[take + lane][2];
+        h = bt->ch[take + lane];
+        q = bt->cp[take + lane];
+    }
+    __syncwarp();
+    if (lane < rest) {
+        bt->cg[lane][0] = a;
+        bt->cg[lane][1] = b;
+        bt->cg[lane][2] = c;
+        bt->ch[lane] = h;
+        bt->cp[lane] = q;
+    }
+    __syncwarp();
+    if (lane == 0) bt->cn = rest;
+    __syncwarp();
+}
 
 // The lookups of `take` queued hkl (slot = lane), warp-cooperatively: the
 // cell rows of all of them are flattened across the lanes, then the g of
@@ -450,19 +493,29 @@ __device__ __forceinline__ void lookup_batch(const volatile WarpPlan* wp, Batch*
             const int rj = owner(gexcl, f);
             const int pos = f + __shfl_sync(0xffffffffu, off, rj);
             const int qq = __shfl_sync(0xffffffffu, qj, rj);
+            bool inb = false;
+            double g0 = 0., g1 = 0., g2 = 0.;
             if (f < gtotal) {
-                const double g0 = __ldg(gs + 3 * (int64_t)pos), g1 = __ldg(gs + 3 * (int64_t)pos + 1),
-                             g2 = __ldg(gs + 3 * (int64_t)pos + 2);
-                const double c0 = bt->c[qq][0], c1 = bt->c[qq][1], c2 = bt->c[qq][2];
-                if (fabs(g0 - c0) <= w0 && fabs(g1 - c1) <= w1 && fabs(g2 - c2) <= w2) {
-                    double u[9], ih[3], hkl[3];
-#pragma unroll
-                    for (int e = 0; e < 9; e++) u[e] = wp->u[e];
-                    const double sv = drlv2_exact(u, g0, g1, g2, ih);
-                    unpack_hkl(bt->hkl[qq], hkl);
-                    act(pos, sv, ih[0] == hkl[0] && ih[1] == hkl[1] && ih[2] == hkl[2]);
-                }
+                g0 = __ldg(gs + 3 * (int64_t)pos);
+                g1 = __ldg(gs + 3 * (int64_t)pos + 1);
+                g2 = __ldg(gs + 3 * (int64_t)pos + 2);
+                inb = fabs(g0 - bt->c[qq][0]) <= w0 && fabs(g1 - bt->c[qq][1]) <= w1 &&
+                      fabs(g2 - bt->c[qq][2]) <= w2;
             }
+            const unsigned mk = __ballot_sync(0xffffffffu, inb);
+            const int cn = bt->cn;  // < 32 here
+            if (inb) {
+                const int slot = cn + __popc(mk & ((1u << lane) - 1u));
+                bt->cg[slot][0] = g0;
+                bt->cg[slot][1] = g1;
+                bt->cg[slot][2] = g2;
+                bt->ch[slot] = bt->hkl[qq];
+                bt->cp[slot] = pos;
+            }
+            __syncwarp();
+            if (lane == 0) bt->cn = cn + __popc(mk);
+            __syncwarp();
+            if (cn + __popc(mk) >= 32) eval_candidates(wp, bt, 32, lane, act);
         }
     }
     __syncwarp();
@@ -514,6 +567,8 @@ __device__ __forceinline__ void walk(volatile WarpPlan* wp, Batch* bt, unsigned 
         return;
     }
     int qn = 0;  // queued (uniform)
+    if (lane == 0) bt->cn = 0;
+    __syncwarp();
     const unsigned lt = (1u << lane) - 1u;
     const int nh0 = wp->nh[0];
     const int64_t nhk = (int64_t)nh0 * wp->nh[1];
@@ -585,6 +640,8 @@ __device__ __forceinline__ void walk(volatile WarpPlan* wp, Batch* bt, unsigned 
         }
     }
     if (qn > 0) lookup_batch(wp, bt, q_w, qn, lane, H, start, gs, act);
+    const int cn = bt->cn;
+    if (cn > 0) eval_candidates(wp, bt, cn, lane, act);
 }
 
 template <int NT>

@@ -132,6 +132,41 @@ def grid_measure(torch, dev, ps, ubis, steps=5, flush=None, check_counts=None, c
             "plain_scan_ubis": st["fallback_ubis"], "counts_equal_score_batch": same}
 
 
+def update_geometry_measure(torch, dev, n_peaks=10_000_000, steps=5, flush=None):
+    """Detector positions -> lab positions -> tth, eta, ds, g for n_peaks: the
+    fused pass against compute_xlylzl + compute_geometry launched in turn
+    (inputs resident, L2 flushed between steps)."""
+    from imaged11_b200 import transform
+    rng = np.random.default_rng(SEED + 11)
+    pars = {"y_center": 1024.3, "z_center": 1021.7, "y_size": 75.0, "z_size": 75.0,
+            "distance": 152300.0, "wavelength": 0.2846, "omegasign": 1.0, "tilt_x": 0.004,
+            "tilt_y": -0.002, "tilt_z": 0.006, "o11": 1, "o12": 0, "o21": 0, "o22": -1,
+            "wedge": 0.01, "chi": 0.02}
+    ct = transform.Ctransform(pars)
+    sc = torch.tensor(rng.uniform(0, 2048, n_peaks), device=dev)
+    fc = torch.tensor(rng.uniform(0, 2048, n_peaks), device=dev)
+    om = torch.tensor(rng.uniform(0, 360, n_peaks), device=dev)
+    xyz = torch.empty((n_peaks, 3), dtype=torch.float64, device=dev)
+    out = torch.empty((n_peaks, 6), dtype=torch.float64, device=dev)
+    t = (5.0, -3.0, 2.0)
+
+    def fused():
+        ct.sf2geometry(sc, fc, om, *t)
+
+    def separate():
+        ct.sf2xyz(sc, fc, out=xyz)
+        ct.xyz2geometry(xyz, om, *t, out=out)
+    for _ in range(3):
+        fused()
+        separate()
+    mf = float(np.mean(cuda_time_ms(torch, fused, steps, flush)))
+    ms = float(np.mean(cuda_time_ms(torch, separate, steps, flush)))
+    return {"case": "update_geometry", "peaks": n_peaks, "fused_ms": mf, "separate_ms": ms,
+            "fused_gbs": 96.0 * n_peaks / (mf * 1e-3) / 1e9,
+            "separate_gbs": 120.0 * n_peaks / (ms * 1e-3) / 1e9,
+            "bytes_per_peak": {"fused": 96, "separate": 120}}
+
+
 def refine_workload(seed=SEED + 7, ngrains=2000):
     """Uneven per-grain refinement: hcp Ti grains (a=2.95, c=4.68 A), per-grain
     peak counts log-uniform in 20..2000 set by a per-grain |g| cutoff (capped by
@@ -248,10 +283,13 @@ def adjoint_measure(torch, dev, steps=5, refine=True):
 
 def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5):
     """Full-scale scan: 20,000 grains (70% hcp Ti, 30% bcc beta-Ti, |g| <= 1.27,
-    15% noise peaks, cfg3 geometry) -> compute_xlylzl + compute_gv (FP64, fused
-    FP32 copy) -> batched scoring of n_ubi trial UBIs -> `rounds` rounds of
-    per-grain refinement (peaks grouped by their simulated grain) -> one
-    residual gradient over 12 geometry parameters + every UBI."""
+    15% noise peaks, cfg3 geometry), end to end on the device:
+    compute_xlylzl + compute_gv -> cell index + scoring of n_ubi trial UBIs ->
+    batched score_and_assign of every peak to the 20,000 grains (their UBIs
+    0.2 deg / 0.2% off truth) -> peaks grouped by label -> `rounds` rounds of
+    per-grain refinement -> hkl of the assigned peaks from the refined UBIs ->
+    one residual gradient over 12 geometry parameters + every UBI.  The FP32
+    screening kernel on the same trial UBIs is timed beside it."""
     from imaged11_b200 import adjoint, batch, synth
     from imaged11_b200 import cImageD11 as cim
     from imaged11_b200._lib import lib, check
@@ -273,15 +311,16 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5):
     gv = torch.empty((n, 3), dtype=torch.float64, device=dev)
     gs = batch.GvecSet(torch.zeros((n, 3), dtype=torch.float64, device=dev))
     ub_d = torch.tensor(trials, device=dev)
-    idx, off = ps.grain_offsets()
-    idx_d = torch.tensor(idx, device=dev)
     u_ref = synth.perturb_ubis(ps.ubis, 0.2, 0.002, rng)
+    u_ref_d = torch.tensor(u_ref, device=dev)
     stream = torch.cuda.current_stream().cuda_stream
     t_arr = np.array([truth["t_x"], truth["t_y"], truth["t_z"]])
-    peaks = adjoint.PeakTable(ps.s[idx], ps.f[idx], ps.omega[idx], ps.hkl[idx], off, truth)
-    grains = batch.GrainSet(torch.zeros((len(idx), 3), dtype=torch.float64, device=dev), off,
-                            u_ref)
-    ws = batch.BatchWorkspace(len(trials), n, refine=False)
+    gws = torch.empty(lib.id11b_grid_score_workspace_bytes(len(trials), 1), dtype=torch.uint8,
+                      device=dev)
+    cbuf = torch.empty((len(trials), 1), dtype=torch.int32, device=dev)
+    d2 = torch.empty(n, dtype=torch.float64, device=dev)
+    lab = torch.empty(n, dtype=torch.int32, device=dev)
+    out = {}
 
     def run(ev):
         ev[0].record()
@@ -290,36 +329,61 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5):
                                        truth["wavelength"], truth["wedge"], truth["chi"],
                                        t_arr.ctypes.data, gv.data_ptr(), gs.g4.data_ptr(), n,
                                        stream), "compute_gv")
-        gs.gv = gv
-        gs.prepare()
         ev[1].record()
-        c = batch.score_batch(ub_d, gs, [tol], workspace=ws)
+        grid = batch.GvecGrid(gv)
+        batch.score_grid(ub_d, grid, [tol], workspace=gws, out=cbuf)
         ev[2].record()
-        torch.index_select(gv, 0, idx_d, out=grains.gv)
-        grains.ubis.copy_(torch.as_tensor(u_ref.reshape(-1, 9), device=dev))
-        grains.refine(tol, rounds)
+        d2.fill_(2.0)
+        lab.fill_(-1)
+        batch.score_and_assign_grid(u_ref_d, grid, tol, d2, lab)
         ev[3].record()
+        lab_s, order = torch.sort(lab, stable=True)
+        first = int((lab_s < 0).sum().item())
+        order, gl = order[first:], lab_s[first:].long()
+        off = torch.zeros(ng + 1, dtype=torch.int64, device=dev)
+        off[1:] = torch.cumsum(torch.bincount(gl, minlength=ng), 0)
+        grains = batch.GrainSet(gv.index_select(0, order), off, u_ref_d.clone())
+        grains.refine(tol, rounds)
+        ev[4].record()
+        ub_pk = grains.ubis.view(-1, 3, 3).index_select(0, gl)
+        hkl = torch.round(torch.einsum("nij,nj->ni", ub_pk, grains.gv))
+        peaks = adjoint.PeakTable(s_d.index_select(0, order), f_d.index_select(0, order),
+                                  om_d.index_select(0, order), hkl, off, truth)
         pt = adjoint.params_tensor(truth).requires_grad_(True)
         ut = grains.ubis.view(-1, 3, 3).clone().requires_grad_(True)
         adjoint.loss(pt, ut, peaks).backward()
-        ev[4].record()
-        ev[4].synchronize()
-        return c
+        ev[5].record()
+        ev[5].synchronize()
+        out.update(assigned=int(n - first), refined_peaks=grains.peaks,
+                   npk_median=int(grains.npk.median().item()))
 
-    run([torch.cuda.Event(enable_timing=True) for _ in range(5)])   # warm-up (module loads)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-    counts = run(ev)
-    names = ["compute_xlylzl+compute_gv", "score_batch", "refine_csr", "adjoint_gradient"]
-    stages = {}
-    for i, nm in enumerate(names):
-        stages[nm] = ev[i].elapsed_time(ev[i + 1])
-    pairs = n_ubi * n + rounds * grains.peaks + peaks.n
+    run([torch.cuda.Event(enable_timing=True) for _ in range(6)])   # warm-up (module loads)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    run(ev)
+    names = ["compute_xlylzl+compute_gv", "cell_index+score_grid", "score_and_assign",
+             "group+refine_csr", "adjoint_gradient"]
+    stages = {nm: ev[i].elapsed_time(ev[i + 1]) for i, nm in enumerate(names)}
+    # the FP32 screening kernel on the same trial UBIs, for comparison
+    gs.gv = gv
+    gs.prepare()
+    ws = batch.BatchWorkspace(len(trials), n, refine=False)
+    c32 = batch.score_batch(ub_d, gs, [tol], workspace=ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    c32 = batch.score_batch(ub_d, gs, [tol], workspace=ws)
+    e1.record()
+    e1.synchronize()
+    pairs = len(trials) * n + ng * n + rounds * out["refined_peaks"] + out["refined_peaks"]
     device_ms = sum(stages.values())
     return {"grains": ng, "peaks": n, "trial_ubis": int(len(trials)), "tol": tol,
             "stage_ms": stages, "pairs": pairs, "device_ms": device_ms,
             "value": pairs / (device_ms * 1e-3), "unit": "pairs/s",
-            "trial_counts_median_max": [int(counts[:, 0].median().item()),
-                                        int(counts[:, 0].max().item())]}
+            "assigned_peaks": out["assigned"], "peaks_per_grain_median": out["npk_median"],
+            "score_batch_fp32_ms": e0.elapsed_time(e1),
+            "score_grid_counts_equal_fp32": bool(torch.equal(c32, cbuf)),
+            "trial_counts_median_max": [int(cbuf[:, 0].median().item()),
+                                        int(cbuf[:, 0].max().item())],
+            "note": "wall between events: host glue (grouping, GrainSet, PeakTable) included"}
 
 
 def workload(rank=0, n_ubi=N_UBI):
@@ -484,6 +548,9 @@ def run_ours(args, rank, world, local_rank):
         for cell in (args.cell or [None]):
             print(json.dumps(grid_measure(torch, dev, ps, ubis, steps=args.steps, cell=cell)))
         return 0
+    if args.case == "geometry":  # fused detector -> geometry pass (profiling case)
+        print(json.dumps(update_geometry_measure(torch, dev, args.peaks, args.steps)))
+        return 0
     if args.case == "gv":       # compute_gv alone (profiling case)
         gbs, ms = compute_gv_measure(torch, ps, dev, args.peaks, args.steps)
         print(json.dumps({"case": "compute_gv", "peaks": args.peaks, "GB/s": gbs, "ms": ms}))
@@ -643,7 +710,7 @@ def main():
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed steps of the scoring step (profiling case)")
     ap.add_argument("--case", default="score",
-                    choices=["score", "gv", "grid", "refine", "adjoint", "pipeline"],
+                    choices=["score", "gv", "geometry", "grid", "refine", "adjoint", "pipeline"],
                     help="gv: compute_gv alone on --peaks lab positions; refine: per-grain "
                          "CSR refinement alone (profiling cases)")
     ap.add_argument("--peaks", type=int, default=10_000_000)

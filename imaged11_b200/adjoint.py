@@ -87,10 +87,14 @@ class PeakTable:
         dev = "cuda"
 
         def f64(a):
+            if torch.is_tensor(a):
+                return a.to(dev, torch.float64).contiguous()
             return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
 
         self.sc, self.fc, self.omega = f64(sc), f64(fc), f64(omega)
-        self.hkl = f64(np.asarray(hkl).reshape(-1, 3))
+        self.hkl = f64(hkl).reshape(-1, 3)
+        if torch.is_tensor(offsets):
+            offsets = offsets.cpu().numpy()
         off = np.ascontiguousarray(offsets, dtype=np.int64)
         self.offsets = torch.as_tensor(off, device=dev)
         self.ngrains = len(off) - 1

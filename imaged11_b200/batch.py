@@ -300,6 +300,8 @@ class GrainSet:
     def __init__(self, gv, offsets, ubis, threads=None):
         torch = _torch()
         self.gv = _dev(gv, torch.float64).reshape(-1, 3)
+        if torch.is_tensor(offsets):
+            offsets = offsets.cpu().numpy()
         off = np.ascontiguousarray(offsets, dtype=np.int64)
         self.ngrains = len(off) - 1
         dev = self.gv.device

@@ -240,7 +240,9 @@ __device__ __forceinline__ uint64_t drlv2_pair(const uint64_t up[9], uint64_t gx
 }
 
 // ------------------------------------------------------------ main kernel --
-template <int R, int NT, int MODE>
+// SUMS = false (MODE_SCORE without a sums output): the rare path counts only
+// and the float sums are not even allocated.
+template <int R, int NT, int MODE, bool SUMS = true>
 __global__ void __launch_bounds__(kBT, MODE == MODE_SCORE ? score_ctas_per_sm(R) : 2)
 k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ g4,
         const double* __restrict__ gv, const double* __restrict__ ubis, int64_t n, int gsplit,
@@ -290,7 +292,7 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 s_cnt[j * (kBT * R) + r * kBT + tid] = 0;
-                s_sum[j * (kBT * R) + r * kBT + tid] = 0.f;
+                if (SUMS) s_sum[j * (kBT * R) + r * kBT + tid] = 0.f;  // absent otherwise
             }
     } else {
         for (int f = 0; f < 17; f++)
@@ -346,7 +348,7 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
                             const int slot = j * (kBT * R) + r * kBT + tid;
                             if (s[r] < band.lo[j]) {
                                 s_cnt[slot]++;
-                                s_sum[slot] += s[r];
+                                if (SUMS) s_sum[slot] += s[r];
                             } else if (s[r] < band.hi[j]) {
                                 double uu[9], ihd[3];
 #pragma unroll
@@ -356,7 +358,7 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
                                 atomicAdd(&ui->nrecheck, 1ull);
                                 if (s64 < tols.t[j] * tols.t[j]) {
                                     s_cnt[slot]++;
-                                    s_sum[slot] += (float)s64;
+                                    if (SUMS) s_sum[slot] += (float)s64;
                                 }
                             }
                         }
@@ -420,7 +422,7 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
                 const int slot = j * (kBT * R) + r * kBT + tid;
                 if (s_cnt[slot]) {
                     atomicAdd(counts + mi[r] * NT + j, s_cnt[slot]);
-                    if (sums) atomicAdd(sums + mi[r] * NT + j, (double)s_sum[slot]);
+                    if (SUMS && sums) atomicAdd(sums + mi[r] * NT + j, (double)s_sum[slot]);
                 }
             }
         }
@@ -579,7 +581,7 @@ static UbiWs ubi_ws_layout(void* base, int64_t m, int64_t n, int mode) {
     return w;
 }
 
-template <int R, int NT, int MODE>
+template <int R, int NT, int MODE, bool SUMS = true>
 static void launch_batch(int64_t m, int64_t n, int gsplit, const float4* packs, const float4* g4,
                          const double* gv, const double* ubis, const Tols& tols,
                          const GvecInfo* gi, UbiInfo* ui, int* counts, double* sums,
@@ -587,8 +589,8 @@ static void launch_batch(int64_t m, int64_t n, int gsplit, const float4* packs, 
     static_assert(MODE == MODE_SCORE || R == 2, "refinement keeps two UBIs per thread");
     const int64_t ublocks = (m + kBT * R - 1) / (kBT * R);
     size_t dyn = MODE == MODE_REFINE ? sizeof(double) * 17 * kBT * R
-                                     : (sizeof(int) + sizeof(float)) * NT * kBT * R;
-    auto kern = k_batch<R, NT, MODE>;
+                                     : (sizeof(int) + (SUMS ? sizeof(float) : 0)) * NT * kBT * R;
+    auto kern = k_batch<R, NT, MODE, SUMS>;
     // static (32 KB of tiles) + dynamic exceeds the 48 KB default: opt in once
     static bool attr_set = false;
     if (!attr_set) {
@@ -684,11 +686,20 @@ template <int R>
 static void launch_score(int ntol, int64_t m, int64_t n, int gsplit, const UbiWs& w,
                          const float4* g4, const double* gv, const double* ubis, const Tols& T,
                          const GvecInfo* gi, int* counts, double* sums, cudaStream_t st) {
-    switch (ntol) {
-        case 1: launch_batch<R, 1, MODE_SCORE>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
-        case 2: launch_batch<R, 2, MODE_SCORE>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
-        case 3: launch_batch<R, 3, MODE_SCORE>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
-        default: launch_batch<R, 4, MODE_SCORE>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
+    if (sums) {
+        switch (ntol) {
+            case 1: launch_batch<R, 1, MODE_SCORE, true>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
+            case 2: launch_batch<R, 2, MODE_SCORE, true>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
+            case 3: launch_batch<R, 3, MODE_SCORE, true>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
+            default: launch_batch<R, 4, MODE_SCORE, true>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
+        }
+    } else {
+        switch (ntol) {
+            case 1: launch_batch<R, 1, MODE_SCORE, false>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, nullptr, nullptr, st); break;
+            case 2: launch_batch<R, 2, MODE_SCORE, false>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, nullptr, nullptr, st); break;
+            case 3: launch_batch<R, 3, MODE_SCORE, false>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, nullptr, nullptr, st); break;
+            default: launch_batch<R, 4, MODE_SCORE, false>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, nullptr, nullptr, st); break;
+        }
     }
 }
 

@@ -351,3 +351,31 @@ class GrainSet:
         with torch.cuda.graph(graph):
             self._launch(tol, iters, 1, self.threads)
         return graph
+
+
+def refine_translations(xyz, omega, offsets, ubis, translations, omegasign, wavelength, wedge,
+                        chi, tol=1.0, iters=20):
+    """Per-grain translations minimising the objective of
+    ImageD11/refinegrains.py refinepositions (the grain's UBI fixed, its
+    assigned peaks' drlv2 summed below tol^2 -- 1.0 there), for all grains in
+    one launch by damped Gauss-Newton.  xyz (n,3) lab positions and omega (n,)
+    sorted by grain, offsets (ngrains+1,), ubis (ngrains,3,3), translations
+    (ngrains,3) starting values.  Returns (translations, cost, npk) as CUDA
+    tensors; iters=0 only evaluates the objective."""
+    torch = _torch()
+    x = _dev(xyz, torch.float64).reshape(-1, 3)
+    om = _dev(omega, torch.float64).reshape(-1)
+    off = _dev(offsets, torch.int64).reshape(-1)
+    u = _dev(ubis, torch.float64).reshape(-1, 9)
+    ng = off.numel() - 1
+    t = _dev(translations, torch.float64).reshape(-1, 3).clone()
+    if u.shape[0] != ng or t.shape[0] != ng or x.shape[0] != om.shape[0]:
+        raise ValueError("refine_translations: inconsistent sizes")
+    cost = torch.empty(ng, dtype=torch.float64, device=x.device)
+    npk = torch.empty(ng, dtype=torch.int32, device=x.device)
+    check(lib.id11b_dev_refine_translations(x.data_ptr(), om.data_ptr(), off.data_ptr(), ng,
+                                            u.data_ptr(), t.data_ptr(), float(omegasign),
+                                            float(wavelength), float(wedge), float(chi),
+                                            float(tol), int(iters), cost.data_ptr(),
+                                            npk.data_ptr(), _stream()), "refine_translations")
+    return t, cost, npk

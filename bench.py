@@ -238,6 +238,69 @@ CFG3_TRUTH = dict(distance=152300., y_center=1024 + 3.7, z_center=1024 - 2.1, ti
                   tilt_y=-0.002, tilt_z=0.006, wedge=0.01, chi=0.02, t_x=5., t_y=-3., t_z=2.)
 
 
+def translations_measure(torch, dev, steps=5, cpu=True):
+    """Per-grain translation refinement (the refinepositions objective): 500
+    FCC Al grains, |g| <= 1.75, each at its own position (uniform +-60 um),
+    0.5 px / 0.05 deg noise, UBIs fixed at truth, start at t = 0, 30
+    iterations, all grains in one launch; the reference's method (a
+    Nelder-Mead simplex on the oracle's compute_gv + score_and_refine, as
+    refinegrains.gof) on a few grains on the host for comparison."""
+    from imaged11_b200 import batch, synth
+    from imaged11_b200 import cImageD11 as cim
+    truth = synth.default_geometry(**CFG3_TRUTH)
+    ps = synth.simulate(500, "Al", gmax=1.75, seed=SEED + 17, geo=truth, noise_frac=0.0,
+                        translations_um=60.0)
+    idx, off = ps.grain_offsets()
+    p, r, dist = synth.xlylzl_params(truth)
+    s_d = torch.tensor(ps.s[idx], device=dev)
+    f_d = torch.tensor(ps.f[idx], device=dev)
+    om = torch.tensor(ps.omega[idx], device=dev)
+    xyz = torch.empty((len(idx), 3), dtype=torch.float64, device=dev)
+    cim.compute_xlylzl(s_d, f_d, p, r.ravel(), dist, xyz)
+    ng = len(off) - 1
+    z = np.zeros((ng, 3))
+
+    def run():
+        return batch.refine_translations(xyz, om, off, ps.ubis, z, truth["omegasign"],
+                                         truth["wavelength"], truth["wedge"], truth["chi"],
+                                         iters=30)
+    for _ in range(3):
+        run()
+    ms = float(np.mean(cuda_time_ms(torch, run, steps)))
+    t, cost, npk = run()
+    err = np.abs(t.cpu().numpy() - ps.translations)
+    out = {"grains": ng, "peaks": int(off[-1]), "iterations": 30, "ms": ms,
+           "grains_per_s": ng / (ms * 1e-3),
+           "error_um_median_max": [float(np.median(err)), float(err.max())]}
+    if cpu:
+        from scipy.optimize import minimize
+        from oracle import oracle as orcm
+        orc = orcm.Reference() if orcm.have_reference() else orcm.Oracle()
+        xyz_h = xyz.cpu().numpy()
+        om_h = ps.omega[idx]
+        t0 = time.perf_counter()
+        nev = 0
+        k = 8
+        for g in range(k):
+            a, b = off[g], off[g + 1]
+
+            def gof(tt, a=a, b=b, g=g):
+                gv = orc.compute_gv(xyz_h[a:b], om_h[a:b], truth["omegasign"],
+                                    truth["wavelength"], truth["wedge"], truth["chi"], tt)
+                n, mean, _ = orc.score_and_refine(ps.ubis[g], gv, 1.0)
+                return n * mean
+            res = minimize(gof, np.zeros(3), method="Nelder-Mead",
+                           options={"xatol": 1e-3, "fatol": 1e-12, "maxiter": 2000})
+            nev += res.nfev
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": k / dt, "unit": "grains/s", "cores": orc.max_threads(),
+                               "kind": "reference" if isinstance(orc, orcm.Reference) else "port",
+                               "sample": "Nelder-Mead on %d grains, %d objective evaluations"
+                                         % (k, nev)}
+        out["ratio_vs_cpu_nelder_mead"] = out["grains_per_s"] / (k / dt)
+    return out
+
+
 def adjoint_measure(torch, dev, steps=5, refine=True):
     """Joint grain + geometry refinement workload: 500 FCC Al grains (~325k
     peaks, |g| <= 1.75) simulated with tilts, wedge, chi, translation and
@@ -548,6 +611,9 @@ def run_ours(args, rank, world, local_rank):
         for cell in (args.cell or [None]):
             print(json.dumps(grid_measure(torch, dev, ps, ubis, steps=args.steps, cell=cell)))
         return 0
+    if args.case == "translations":  # per-grain translation refinement
+        print(json.dumps(translations_measure(torch, dev, steps=args.steps)))
+        return 0
     if args.case == "geometry":  # fused detector -> geometry pass (profiling case)
         print(json.dumps(update_geometry_measure(torch, dev, args.peaks, args.steps)))
         return 0
@@ -633,6 +699,7 @@ def run_ours(args, rank, world, local_rank):
     refine = refine_csr_measure(torch, dev, steps=max(3, args.steps), flush=flush,
                                 cpu=(world == 1))
     adj = adjoint_measure(torch, dev, steps=max(3, args.steps))
+    trans = translations_measure(torch, dev, steps=max(3, args.steps), cpu=(world == 1))
     # the same scoring through the reciprocal-space cell index (exact FP64 lookups)
     cell = grid_measure(torch, dev, ps, ubis, steps=max(3, args.steps), flush=flush,
                         check_counts=counts)
@@ -687,6 +754,7 @@ def run_ours(args, rank, world, local_rank):
         "cell_index": cell,
         "refine_csr": refine,
         "adjoint": adj,
+        "translations": trans,
         "compute_gv": {"peaks": 10_000_000, "ms": gv_ms, "achieved_gbs": gv_gbs,
                        "peak_gbs": hbm_peak, "peak_kind": hbm_kind,
                        "frac": gv_gbs / hbm_peak, "bytes_per_peak": 56},
@@ -710,7 +778,8 @@ def main():
     ap.add_argument("--kernel-only", action="store_true",
                     help="only warm-up + timed steps of the scoring step (profiling case)")
     ap.add_argument("--case", default="score",
-                    choices=["score", "gv", "geometry", "grid", "refine", "adjoint", "pipeline"],
+                    choices=["score", "gv", "geometry", "grid", "translations", "refine", "adjoint",
+                             "pipeline"],
                     help="gv: compute_gv alone on --peaks lab positions; refine: per-grain "
                          "CSR refinement alone (profiling cases)")
     ap.add_argument("--peaks", type=int, default=10_000_000)

@@ -68,7 +68,8 @@ def compute_gv_measure(torch, ps, dev, n_peaks=10_000_000, steps=5, flush=None):
     return 56.0 * n_peaks / (ms * 1e-3) / 1e9, ms
 
 
-def grid_measure(torch, dev, ps, ubis, steps=5, flush=None, check_counts=None, cell=None):
+def grid_measure(torch, dev, ps, ubis, steps=5, flush=None, check_counts=None, cell=None,
+                 xsub=None):
     """Scoring through the reciprocal-space cell index on the same workload:
     index build time, ms per score_grid call (inputs resident, L2 flushed
     between calls) and pairs decided per second."""
@@ -76,10 +77,10 @@ def grid_measure(torch, dev, ps, ubis, steps=5, flush=None, check_counts=None, c
     gv_d = torch.tensor(ps.gv, device=dev)
     ubis_d = torch.tensor(ubis, device=dev)
     m, n, T = len(ubis), len(ps.gv), len(TOLS)
-    batch.GvecGrid(gv_d, cell=cell)                       # load the kernels
+    batch.GvecGrid(gv_d, cell=cell, xsub=xsub)            # load the kernels
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    grid = batch.GvecGrid(gv_d, cell=cell)
+    grid = batch.GvecGrid(gv_d, cell=cell, xsub=xsub)
     torch.cuda.synchronize()
     build_ms = (time.perf_counter() - t0) * 1e3
     ws = torch.empty(batch.lib.id11b_grid_score_workspace_bytes(m, T), dtype=torch.uint8,
@@ -126,7 +127,8 @@ def grid_measure(torch, dev, ps, ubis, steps=5, flush=None, check_counts=None, c
             "assign": {"ubis": m, "tol": 0.05, "ms": t_asg, "value": m * n / (t_asg * 1e-3),
                        "sequential_plain_fp64_value": k * n / (t_seq * 1e-3),
                        "sequential_ubis": k, "identical_to_sequential": same_assign},
-            "build_ms_wall": build_ms, "cells": grid.nx ** 3, "cell_A^-1": grid.cs,
+            "build_ms_wall": build_ms, "cells": grid.nx ** 3 * grid.xsub, "cell_A^-1": grid.cs,
+            "xsub": grid.xsub,
             "pairs_tested_fp64": st["pairs_tested"],
             "tested_fraction": st["pairs_tested"] / float(m * n),
             "plain_scan_ubis": st["fallback_ubis"], "counts_equal_score_batch": same}
@@ -609,7 +611,9 @@ def run_ours(args, rank, world, local_rank):
         return 0
     if args.case == "grid":     # cell-index scoring alone (profiling case)
         for cell in (args.cell or [None]):
-            print(json.dumps(grid_measure(torch, dev, ps, ubis, steps=args.steps, cell=cell)))
+            for xsub in (args.xsub or [None]):
+                print(json.dumps(grid_measure(torch, dev, ps, ubis, steps=args.steps, cell=cell,
+                                              xsub=xsub)))
         return 0
     if args.case == "translations":  # per-grain translation refinement
         print(json.dumps(translations_measure(torch, dev, steps=args.steps)))
@@ -784,6 +788,7 @@ def main():
                          "CSR refinement alone (profiling cases)")
     ap.add_argument("--peaks", type=int, default=10_000_000)
     ap.add_argument("--cell", type=float, nargs="*", help="grid case: cell sides (1/A) to time")
+    ap.add_argument("--xsub", type=int, nargs="*", help="grid case: x subdivisions to time")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

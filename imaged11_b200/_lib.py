@@ -56,15 +56,16 @@ _SIGNATURES = [
                                           _p, _i64, _p]),
     ("id11b_dev_gvec_bounds", _i, [_p, _i64, _p, _p]),
     ("id11b_grid_plan", _i, [ctypes.c_float, _i64, _d, _p, _p]),
-    ("id11b_grid_bytes", _i64, [_i64, _i]),
-    ("id11b_dev_build_grid", _i, [_p, _i64, ctypes.c_float, ctypes.c_float, _d, _i, _p, _i64,
-                                   _p]),
+    ("id11b_grid_bytes", _i64, [_i64, _i, _i]),
+    ("id11b_dev_build_grid", _i, [_p, _i64, ctypes.c_float, ctypes.c_float, _d, _i, _i, _p,
+                                   _i64, _p]),
     ("id11b_grid_score_workspace_bytes", _i64, [_i64, _i]),
-    ("id11b_dev_score_grid", _i, [_p, _i64, _p, _i64, _i, _p, _p, _i, _p, _p, _p, _i64, _p]),
+    ("id11b_dev_score_grid", _i, [_p, _i64, _p, _i64, _i, _i, _p, _p, _i, _p, _p, _p, _i64,
+                                   _p]),
     ("id11b_grid_stats", _i, [_p, _p, _p, _p, _p, _p]),
     ("id11b_assign_workspace_bytes", _i64, [_i64]),
-    ("id11b_dev_score_and_assign_grid", _i, [_p, _i64, _p, _p, _i64, _i, _p, _d, _p, _p, _p, _p,
-                                              _i64, _p]),
+    ("id11b_dev_score_and_assign_grid", _i, [_p, _i64, _p, _p, _i64, _i, _i, _p, _d, _p, _p,
+                                              _p, _p, _i64, _p]),
     ("id11b_dev_refine_batch", _i, [_p, _i64, _p, _p, _i64, _p, _d, _i, _p, _p, _p, _i64, _p]),
     ("id11b_batch_stats", _i, [_p, _i64, _i64, _i, _p, _p, _p, _p]),
     ("id11b_refine_csr_workspace_bytes", _i64, []),

@@ -53,12 +53,13 @@ constexpr double kMaxCond = 1e6;
 constexpr int kMaxParts = 64;
 
 struct Header {
-    double lo, cs, inv_cs;  // cube [lo, lo + nx*cs)^3
+    double lo, cs, inv_cs;  // cube [lo, lo + nx*cs)^3; y and z cells of side cs
+    double inv_csx;         // x cells: side cs / xsub (nxx = nx * xsub of them)
     double rmax;            // max |g| over regular g (rounded up)
     int64_t ncells;
     int64_t n;
     int32_t nx;
-    int32_t pad;
+    int32_t nxx;
     unsigned long long nfallback;  // UBIs scored by the plain scan (last call)
     unsigned long long ntested;    // (UBI, g) pairs evaluated in FP64 (last call)
 };
@@ -106,8 +107,16 @@ __device__ __forceinline__ int coord(double x, const Header& H) {
     return (int)f;
 }
 
+// x is cut finer (a row of cells is one contiguous range whatever its length,
+// so finer x cells cost memory, not lookups)
+__device__ __forceinline__ int coord_x(double x, const Header& H) {
+    double f = __dmul_rn(__dsub_rn(x, H.lo), H.inv_csx);
+    f = fmin(fmax(f, 0.0), (double)(H.nxx - 1));
+    return (int)f;
+}
+
 __device__ __forceinline__ int64_t cell_of(double a, double b, double c, const Header& H) {
-    return ((int64_t)coord(c, H) * H.nx + coord(b, H)) * H.nx + coord(a, H);
+    return ((int64_t)coord(c, H) * H.nx + coord(b, H)) * H.nxx + coord_x(a, H);
 }
 
 // ------------------------------------------------------------------ build --
@@ -462,8 +471,8 @@ __device__ __forceinline__ void lookup_batch(const volatile WarpPlan* wp, Batch*
         bt->hkl[lane] = q;
         const int iy0 = coord(c[1] - wp->w[1], H), iy1 = coord(c[1] + wp->w[1], H);
         const int iz0 = coord(c[2] - wp->w[2], H), iz1 = coord(c[2] + wp->w[2], H);
-        bt->ix0[lane] = coord(c[0] - wp->w[0], H);
-        bt->ix1[lane] = coord(c[0] + wp->w[0], H);
+        bt->ix0[lane] = coord_x(c[0] - wp->w[0], H);
+        bt->ix1[lane] = coord_x(c[0] + wp->w[0], H);
         bt->iy0[lane] = iy0;
         bt->ny[lane] = iy1 - iy0 + 1;
         bt->iz0[lane] = iz0;
@@ -481,7 +490,7 @@ __device__ __forceinline__ void lookup_batch(const volatile WarpPlan* wp, Batch*
         if (rf < rtotal) {
             const int ny = bt->ny[qj];
             const int iy = bt->iy0[qj] + rr % ny, iz = bt->iz0[qj] + rr / ny;
-            const int64_t row = ((int64_t)iz * H.nx + iy) * H.nx;
+            const int64_t row = ((int64_t)iz * H.nx + iy) * H.nxx;
             st = __ldg(start + row + bt->ix0[qj]);
             len = __ldg(start + row + bt->ix1[qj] + 1) - st;
         }
@@ -923,19 +932,24 @@ extern "C" int id11b_grid_plan(float gmax, int64_t n, double cell, int32_t* nx, 
     return ID11B_OK;
 }
 
-extern "C" int64_t id11b_grid_bytes(int64_t n, int32_t nx) {
-    if (n < 0 || nx < 1) return -1;
-    return (int64_t)layout(n, (int64_t)nx * nx * nx).bytes;
+static bool grid_dims_ok(int32_t nx, int32_t xsub) {
+    return nx >= 1 && nx <= 400 && xsub >= 1 && xsub <= 16 && (int64_t)nx * nx * nx * xsub <= (1 << 26);
+}
+
+extern "C" int64_t id11b_grid_bytes(int64_t n, int32_t nx, int32_t xsub) {
+    if (n < 0 || !grid_dims_ok(nx, xsub)) return -1;
+    return (int64_t)layout(n, (int64_t)nx * nx * nx * xsub).bytes;
 }
 
 extern "C" int id11b_dev_build_grid(const double* gv, int64_t n, float gmax, float rmax, double cs,
-                                    int32_t nx, void* gridbuf, int64_t grid_bytes, void* stream) {
-    if (n < 0 || nx < 1 || nx > 400 || !gridbuf || (n > 0 && !gv) || !(cs > 0.) ||
+                                    int32_t nx, int32_t xsub, void* gridbuf, int64_t grid_bytes,
+                                    void* stream) {
+    if (n < 0 || !grid_dims_ok(nx, xsub) || !gridbuf || (n > 0 && !gv) || !(cs > 0.) ||
         !(gmax >= 0.f) || !(rmax >= 0.f))
         return ID11B_ERR_ARG;
     if ((uintptr_t)gridbuf & 255) return ID11B_ERR_ALIGN;
     if (n > INT32_MAX - 1) return ID11B_ERR_SIZE;
-    const int64_t ncells = (int64_t)nx * nx * nx;
+    const int64_t ncells = (int64_t)nx * nx * nx * xsub;
     const Layout L = layout(n, ncells);
     if (grid_bytes < (int64_t)L.bytes) return ID11B_ERR_SIZE;
     cudaStream_t st = (cudaStream_t)stream;
@@ -945,10 +959,12 @@ extern "C" int id11b_dev_build_grid(const double* gv, int64_t n, float gmax, flo
     h.lo = -((double)gmax * (1. + 1e-6) + 1e-300);
     h.cs = cs;
     h.inv_cs = 1.0 / cs;
+    h.inv_csx = (double)xsub / cs;
     h.rmax = (double)rmax;
     h.ncells = ncells;
     h.n = n;
     h.nx = nx;
+    h.nxx = nx * xsub;
     static_assert(sizeof(Header) <= 256, "header");
     // a copy from pageable memory returns once the source has been staged,
     // so the stack value may go out of scope
@@ -988,11 +1004,12 @@ extern "C" int64_t id11b_grid_score_workspace_bytes(int64_t m, int ntol) {
 }
 
 extern "C" int id11b_dev_score_grid(const double* ubis, int64_t m, const double* gv, int64_t n,
-                                    int32_t nx, const void* gridbuf, const double* tols_host,
-                                    int ntol, int32_t* counts, double* sums, void* ws,
-                                    int64_t ws_bytes, void* stream) {
-    if (!tols_host || ntol < 1 || ntol > ID11B_MAX_TOLS || m < 0 || n < 0 || nx < 1 ||
-        nx > 400 || !gridbuf || !ws || (m > 0 && (!ubis || !counts)) || (n > 0 && !gv))
+                                    int32_t nx, int32_t xsub, const void* gridbuf,
+                                    const double* tols_host, int ntol, int32_t* counts,
+                                    double* sums, void* ws, int64_t ws_bytes, void* stream) {
+    if (!tols_host || ntol < 1 || ntol > ID11B_MAX_TOLS || m < 0 || n < 0 ||
+        !grid_dims_ok(nx, xsub) || !gridbuf || !ws || (m > 0 && (!ubis || !counts)) ||
+        (n > 0 && !gv))
         return ID11B_ERR_ARG;
     Tols T;
     for (int j = 0; j < ID11B_MAX_TOLS; j++) T.t[j] = j < ntol ? tols_host[j] : 0.;
@@ -1002,7 +1019,7 @@ extern "C" int id11b_dev_score_grid(const double* ubis, int64_t m, const double*
     if (ws_bytes < id11b_grid_score_workspace_bytes(m, ntol)) return ID11B_ERR_SIZE;
     if (m > INT32_MAX) return ID11B_ERR_SIZE;
     cudaStream_t st = (cudaStream_t)stream;
-    const Layout L = layout(n, (int64_t)nx * nx * nx);
+    const Layout L = layout(n, (int64_t)nx * nx * nx * xsub);
     char* b = (char*)gridbuf;
     Header* H = (Header*)b;
     ID11B_CHECK(cudaMemsetAsync(&H->nfallback, 0, 2 * sizeof(unsigned long long), st));
@@ -1058,11 +1075,11 @@ extern "C" int64_t id11b_assign_workspace_bytes(int64_t n) {
 
 extern "C" int id11b_dev_score_and_assign_grid(const double* ubis, int64_t m,
                                                const int32_t* grain_labels, const double* gv,
-                                               int64_t n, int32_t nx, const void* gridbuf,
-                                               double tol, double* drlv2, int32_t* labels,
-                                               int32_t* npk, void* ws, int64_t ws_bytes,
-                                               void* stream) {
-    if (m < 0 || n < 0 || nx < 1 || nx > 400 || !gridbuf || !ws || (m > 0 && !ubis) ||
+                                               int64_t n, int32_t nx, int32_t xsub,
+                                               const void* gridbuf, double tol, double* drlv2,
+                                               int32_t* labels, int32_t* npk, void* ws,
+                                               int64_t ws_bytes, void* stream) {
+    if (m < 0 || n < 0 || !grid_dims_ok(nx, xsub) || !gridbuf || !ws || (m > 0 && !ubis) ||
         (n > 0 && (!gv || !drlv2 || !labels)) || !(tol >= 0.) || !(tol < 1e3))
         return ID11B_ERR_ARG;
     if (((uintptr_t)gridbuf & 255) || ((uintptr_t)ws & 255)) return ID11B_ERR_ALIGN;
@@ -1071,7 +1088,7 @@ extern "C" int id11b_dev_score_and_assign_grid(const double* ubis, int64_t m,
     cudaStream_t st = (cudaStream_t)stream;
     if (npk && m > 0) ID11B_CHECK(cudaMemsetAsync(npk, 0, sizeof(int32_t) * (size_t)m, st));
     if (m == 0 || n == 0) return ID11B_OK;
-    const int64_t ncells = (int64_t)nx * nx * nx;
+    const int64_t ncells = (int64_t)nx * nx * nx * xsub;
     const Layout L = layout(n, ncells);
     const char* b = (const char*)gridbuf;
     const Header* H = (const Header*)b;

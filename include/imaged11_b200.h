@@ -241,8 +241,9 @@ int id11b_dev_score_batch_tiled(const double *ubis, int64_t m, const double *gv,
  *      regular g, as float bits rounded up (device, 2 x uint32);
  *   2. id11b_grid_plan (host): nx and cs for n g-vectors; cell = 0 picks about
  *      one g per cell of the cube, else the requested side (nx <= 400);
- *   3. id11b_dev_build_grid into gridbuf (id11b_grid_bytes(n, nx), 256-byte
- *      aligned).
+ *   3. id11b_dev_build_grid into gridbuf (id11b_grid_bytes(n, nx, xsub),
+ *      256-byte aligned): y and z cut into nx cells of side cs, x into
+ *      nx * xsub cells of side cs / xsub (xsub 1..16, nx^3 * xsub <= 2^26).
  * id11b_dev_score_grid then gives the counts (and optional sums of drlv2) of
  * id11b_dev_score_batch, identical to the reference's score() for every
  * (UBI, tol): every candidate pair is evaluated in the reference's FP64
@@ -253,12 +254,13 @@ int id11b_dev_score_batch_tiled(const double *ubis, int64_t m, const double *gv,
  * evaluated. */
 int id11b_dev_gvec_bounds(const double *gv, int64_t n, uint32_t *bounds, void *stream);
 int id11b_grid_plan(float gmax, int64_t n, double cell, int32_t *nx, double *cs);
-int64_t id11b_grid_bytes(int64_t n, int32_t nx);
+int64_t id11b_grid_bytes(int64_t n, int32_t nx, int32_t xsub);
 int id11b_dev_build_grid(const double *gv, int64_t n, float gmax, float rmax, double cs,
-                         int32_t nx, void *gridbuf, int64_t grid_bytes, void *stream);
+                         int32_t nx, int32_t xsub, void *gridbuf, int64_t grid_bytes,
+                         void *stream);
 int64_t id11b_grid_score_workspace_bytes(int64_t m, int ntol);
 int id11b_dev_score_grid(const double *ubis, int64_t m, const double *gv, int64_t n, int32_t nx,
-                         const void *gridbuf, const double *tols_host, int ntol,
+                         int32_t xsub, const void *gridbuf, const double *tols_host, int ntol,
                          int32_t *counts, double *sums, void *ws, int64_t ws_bytes,
                          void *stream);
 int id11b_grid_stats(const void *gridbuf, int64_t *nregular, int64_t *nspecial,
@@ -276,7 +278,7 @@ int id11b_grid_stats(const void *gridbuf, int64_t *nregular, int64_t *nspecial,
  * id11b_assign_workspace_bytes(n), 256-byte aligned. */
 int64_t id11b_assign_workspace_bytes(int64_t n);
 int id11b_dev_score_and_assign_grid(const double *ubis, int64_t m, const int32_t *grain_labels,
-                                    const double *gv, int64_t n, int32_t nx,
+                                    const double *gv, int64_t n, int32_t nx, int32_t xsub,
                                     const void *gridbuf, double tol, double *drlv2,
                                     int32_t *labels, int32_t *npk, void *ws, int64_t ws_bytes,
                                     void *stream);

@@ -67,11 +67,12 @@ def test_scene_counts_and_sums(B, oracle, scene, cuda):
     assert np.array_equal(s2.cpu().numpy(), s)
 
 
-@pytest.mark.parametrize("cell", [0.004, 0.03, 0.25, 1.0])
-def test_cell_sizes(B, oracle, scene, cell, cuda):
+@pytest.mark.parametrize("cell,xsub", [(0.004, 4), (0.03, 1), (0.03, 16), (0.25, 3),
+                                       (1.0, 4)])
+def test_cell_sizes(B, oracle, scene, cell, xsub, cuda):
     ps, ubis = scene
     u = ubis[:300]
-    grid = B.GvecGrid(ps.gv, cell=cell)
+    grid = B.GvecGrid(ps.gv, cell=cell, xsub=xsub)
     c = B.score_grid(u, grid, [0.05, 0.1]).cpu().numpy()
     assert np.array_equal(c, oracle.score_many(u, ps.gv, [0.05, 0.1])), cell
 

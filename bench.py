@@ -123,7 +123,18 @@ def grid_measure(torch, dev, ps, ubis, steps=5, flush=None, check_counts=None, c
     same_assign = bool(torch.equal(lab, ref_lab) and torch.equal(d, ref_d))
     t_seq = float(np.mean(cuda_time_ms(torch, lambda: assign_seq(k), 2, flush)))
     t_asg = float(np.mean(cuda_time_ms(torch, lambda: assign(m), steps, flush)))
+    # one round of dense score_and_refine for every trial UBI (tol 0.05): through
+    # the index, and through the FP32-screened refine_batch
+    gs = batch.GvecSet(gv_d)
+    rws = batch.BatchWorkspace(m, n, refine=True)
+    t_rg = float(np.mean(cuda_time_ms(torch, lambda: batch.refine_grid(ubis_d.clone(), grid, 0.05),
+                                      steps, flush)))
+    t_rb = float(np.mean(cuda_time_ms(
+        torch, lambda: batch.refine_batch(ubis_d.clone(), gs, 0.05, workspace=rws), steps,
+        flush)))
     return {"ms": ms, "value": m * n * T / (ms * 1e-3), "unit": "pairs/s",
+            "refine": {"ubis": m, "tol": 0.05, "grid_ms": t_rg, "batch_fp32_ms": t_rb,
+                       "value": m * n / (t_rg * 1e-3), "batch_value": m * n / (t_rb * 1e-3)},
             "assign": {"ubis": m, "tol": 0.05, "ms": t_asg, "value": m * n / (t_asg * 1e-3),
                        "sequential_plain_fp64_value": k * n / (t_seq * 1e-3),
                        "sequential_ubis": k, "identical_to_sequential": same_assign},

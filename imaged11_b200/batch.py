@@ -198,6 +198,25 @@ def score_grid(ubis, grid, tols, sums=False, workspace=None, out=None):
     return (counts, s) if sums else counts
 
 
+def refine_grid(ubis, grid, tol, iters=1):
+    """``iters`` rounds of score_and_refine for every UBI against every g,
+    through the cell index (the result of refine_batch, found by lookup).
+    Returns (ubis (m,3,3) refined, npk, mean drlv2 of the last round's input
+    UBIs) as CUDA tensors; a CUDA float64 input is updated in place."""
+    torch = _torch()
+    u = _dev(ubis, torch.float64).reshape(-1, 9)
+    m = u.shape[0]
+    npk = torch.empty(m, dtype=torch.int32, device=u.device)
+    mean = torch.empty(m, dtype=torch.float64, device=u.device)
+    ws = torch.empty(max(lib.id11b_grid_refine_workspace_bytes(m), 256), dtype=torch.uint8,
+                     device=u.device)
+    check(lib.id11b_dev_refine_grid(u.data_ptr(), m, grid.gv.data_ptr(), grid.n, grid.nx,
+                                    grid.xsub, grid.buf.data_ptr(), float(tol), int(iters),
+                                    npk.data_ptr(), mean.data_ptr(), ws.data_ptr(), ws.numel(),
+                                    _stream()), "refine_grid")
+    return u.view(-1, 3, 3), npk, mean
+
+
 def score_and_assign_grid(ubis, grid, tol, drlv2, labels, grain_labels=None, npk=False):
     """score_and_assign (ImageD11 src/closest.c:366-397) for every grain in
     order, as ImageD11/indexing.py fight_over_peaks calls it, in one pass

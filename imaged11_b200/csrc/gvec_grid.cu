@@ -419,9 +419,10 @@ __device__ __forceinline__ void eval_candidates(const volatile WarpPlan* wp, Bat
         double u[9], ih[3], hkl[3];
 #pragma unroll
         for (int e = 0; e < 9; e++) u[e] = wp->u[e];
-        const double sv = drlv2_exact(u, bt->cg[lane][0], bt->cg[lane][1], bt->cg[lane][2], ih);
+        const double g[3] = {bt->cg[lane][0], bt->cg[lane][1], bt->cg[lane][2]};
+        const double sv = drlv2_exact(u, g[0], g[1], g[2], ih);
         unpack_hkl(bt->ch[lane], hkl);
-        act(bt->cp[lane], sv, ih[0] == hkl[0] && ih[1] == hkl[1] && ih[2] == hkl[2]);
+        act(bt->cp[lane], sv, ih[0] == hkl[0] && ih[1] == hkl[1] && ih[2] == hkl[2], g, ih);
     }
     __syncwarp();
     const int rest = bt->cn - take;  // < 32
@@ -452,7 +453,8 @@ __device__ __forceinline__ void eval_candidates(const volatile WarpPlan* wp, Bat
 // cell rows of all of them are flattened across the lanes, then the g of
 // each 32 rows, so the lanes stay converged whatever the per-query sizes.
 // Every g inside a box is evaluated in the reference's FP64 arithmetic and
-// handed to act(pos, drlv2, own), own = (rounded h == the box's hkl).
+// handed to act(pos, drlv2, own, g, ih), own = (ih, the rounded h, == the
+// box's hkl).
 template <class Act>
 __device__ __forceinline__ void lookup_batch(const volatile WarpPlan* wp, Batch* bt,
                                              const unsigned long long* q_w, int take, int lane,
@@ -557,7 +559,7 @@ __device__ __forceinline__ bool setup_plan(volatile WarpPlan* wp, const double* 
 }
 
 // Every (UBI, g) pair of work item `part` of `parts` whose drlv2 can be below
-// the plan's tolerance goes to act(pos, drlv2, own): through the hkl lookup
+// the plan's tolerance goes to act(pos, drlv2, own, g, ih): through the hkl lookup
 // when ok, else by a plain scan of the regular g (own = true: each g once).
 template <class Act>
 __device__ __forceinline__ void walk(volatile WarpPlan* wp, Batch* bt, unsigned long long* q_w,
@@ -570,8 +572,9 @@ __device__ __forceinline__ void walk(volatile WarpPlan* wp, Batch* bt, unsigned 
         for (int e = 0; e < 9; e++) u[e] = wp->u[e];
         for (int64_t f = (int64_t)part * 32 + lane; f < nreg; f += 32 * (int64_t)parts) {
             double ih[3];
-            const double s = drlv2_exact(u, gs[3 * f], gs[3 * f + 1], gs[3 * f + 2], ih);
-            act((int)f, s, true);
+            const double g[3] = {gs[3 * f], gs[3 * f + 1], gs[3 * f + 2]};
+            const double s = drlv2_exact(u, g[0], g[1], g[2], ih);
+            act((int)f, s, true, g, ih);
         }
         return;
     }
@@ -681,7 +684,7 @@ k_score(const double* __restrict__ ubis, int64_t m, int parts, Header* __restric
     }
     unsigned long long tested = 0;
     const bool ok = setup_plan(s_plan + w, ubis, i, tmax, H, nreg, lane);
-    auto act = [&](int, double s, bool own) {
+    auto act = [&](int, double s, bool own, const double*, const double*) {
         tested++;
         if (own) {
 #pragma unroll
@@ -745,6 +748,110 @@ k_score_finish(const double* __restrict__ ubis, int64_t m, int parts, int ntol, 
     }
 }
 
+// ------------------------------------------------------------ refinement --
+// score_and_refine (ImageD11 src/closest.c:267-345) for many UBIs against all
+// g through the index: the pairs with drlv2 < tol^2 are exactly the ones the
+// lookup hands over with own = true; each adds ih.g^T, ih.ih^T, drlv2 and 1 to
+// the normal equations in the reference's FP64 operations, per lane in shared
+// memory ([field][lane]), then warp trees, per-part partials and a fixed-order
+// finish per UBI that applies the reference's update.
+constexpr int kLsqF = 17;  // R 9 (g_i ih_j at 3i+j), H 6 (00 10 20 11 21 22), sum, n
+
+__device__ __forceinline__ void lsq_add(double* acc, double s, const double* g,
+                                        const double* ih) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) acc[(3 * i + j) * 32] = dadd(acc[(3 * i + j) * 32], dmul(ih[j], g[i]));
+    acc[9 * 32] = dadd(acc[9 * 32], dmul(ih[0], ih[0]));
+    acc[10 * 32] = dadd(acc[10 * 32], dmul(ih[1], ih[0]));
+    acc[11 * 32] = dadd(acc[11 * 32], dmul(ih[2], ih[0]));
+    acc[12 * 32] = dadd(acc[12 * 32], dmul(ih[1], ih[1]));
+    acc[13 * 32] = dadd(acc[13 * 32], dmul(ih[2], ih[1]));
+    acc[14 * 32] = dadd(acc[14 * 32], dmul(ih[2], ih[2]));
+    acc[15 * 32] = dadd(acc[15 * 32], s);
+    acc[16 * 32] += 1.0;
+}
+
+__global__ void __launch_bounds__(kST, ID11B_GRID_MINB)
+k_refine(const double* __restrict__ ubis, int64_t m, int parts, const Header* __restrict__ Hp,
+         const int* __restrict__ start, const double* __restrict__ gs, double tol,
+         double* __restrict__ part_out) {
+    __shared__ unsigned long long s_q[kSW][kQueue];
+    __shared__ WarpPlan s_plan[kSW];
+    __shared__ Batch s_batch[kSW];
+    __shared__ double s_lsq[kSW][kLsqF * 32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t wk = ((int64_t)blockIdx.x * kST + threadIdx.x) >> 5;
+    if (wk >= m * parts) return;  // uniform per warp
+    const int64_t i = wk / parts;
+    const int part = (int)(wk % parts);
+    const Header H = *Hp;
+    const int64_t nreg = start[H.ncells];
+    const double t2 = tol * tol;
+    double* acc = s_lsq[w] + lane;
+#pragma unroll
+    for (int f = 0; f < kLsqF; f++) acc[f * 32] = 0.;
+    const bool ok = setup_plan(s_plan + w, ubis, i, tol, H, nreg, lane);
+    auto act = [&](int, double s, bool own, const double* g, const double* ih) {
+        if (own && s < t2) lsq_add(acc, s, g, ih);
+    };
+    walk(s_plan + w, s_batch + w, s_q[w], ok, part, parts, lane, H, nreg, start, gs, act);
+    __syncwarp();
+#pragma unroll 1
+    for (int f = 0; f < kLsqF; f++) {
+        const double v = warp_sum(acc[f * 32]);
+        if (lane == 0) part_out[(i * parts + part) * kLsqF + f] = v;
+    }
+}
+
+// One thread per UBI: partials in part order, then the g outside the regular
+// range in list order, then the reference's update; n and mean drlv2 of the
+// UBI as it was on entry.
+__global__ void __launch_bounds__(kGT)
+k_refine_finish(double* __restrict__ ubis, int64_t m, int parts, double tol,
+                const double* __restrict__ part_in, const double* __restrict__ gv,
+                const int* __restrict__ special, const int* __restrict__ nspecial,
+                int* __restrict__ npk, double* __restrict__ mean) {
+    const int64_t i = (int64_t)blockIdx.x * kGT + threadIdx.x;
+    if (i >= m) return;
+    double t[kLsqF];
+    for (int f = 0; f < kLsqF; f++) t[f] = 0.;
+    for (int p = 0; p < parts; p++)
+        for (int f = 0; f < kLsqF; f++) t[f] += part_in[(i * parts + p) * kLsqF + f];
+    double u[9];
+    for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
+    const int ns = *nspecial;
+    for (int q = 0; q < ns; q++) {
+        const int64_t k = special[q];
+        double ih[3];
+        const double g[3] = {gv[3 * k], gv[3 * k + 1], gv[3 * k + 2]};
+        const double s = drlv2_exact(u, g[0], g[1], g[2], ih);
+        if (s < tol * tol) {
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) t[3 * a + b] = dadd(t[3 * a + b], dmul(ih[b], g[a]));
+            t[9] = dadd(t[9], dmul(ih[0], ih[0]));
+            t[10] = dadd(t[10], dmul(ih[1], ih[0]));
+            t[11] = dadd(t[11], dmul(ih[2], ih[0]));
+            t[12] = dadd(t[12], dmul(ih[1], ih[1]));
+            t[13] = dadd(t[13], dmul(ih[2], ih[1]));
+            t[14] = dadd(t[14], dmul(ih[2], ih[2]));
+            t[15] = dadd(t[15], s);
+            t[16] += 1.0;
+        }
+    }
+    double R[9], Hm[9];
+    for (int f = 0; f < 9; f++) R[f] = t[f];
+    Hm[0] = t[9];  Hm[1] = t[10]; Hm[2] = t[11];
+    Hm[3] = t[10]; Hm[4] = t[12]; Hm[5] = t[13];
+    Hm[6] = t[11]; Hm[7] = t[13]; Hm[8] = t[14];
+    lsq_update_exact(R, Hm, u);
+    for (int e = 0; e < 9; e++) ubis[9 * i + e] = u[e];
+    const long long n = (long long)t[16];
+    if (npk) npk[i] = (int)n;
+    if (mean) mean[i] = n > 0 ? t[15] / (double)n : 0.;
+}
+
 // ------------------------------------------------------------ assignment --
 // Batched score_and_assign (ImageD11 src/closest.c:366-397) over m grains in
 // order: for each g the reference's sequence of calls leaves the label of the
@@ -770,7 +877,7 @@ k_assign(const double* __restrict__ ubis, int64_t m, int parts, const Header* __
     const int64_t nreg = start[H.ncells];
     const double t2 = tol * tol;
     const bool ok = setup_plan(s_plan + w, ubis, i, tol, H, nreg, lane);
-    auto act = [&](int pos, double s, bool own) {
+    auto act = [&](int pos, double s, bool own, const double*, const double*) {
         if (!own || !(s < t2)) return;
         const int k = __ldg(gidx + pos);
         if (!(s < __ldg(drlv2 + k))) return;
@@ -1112,5 +1219,40 @@ extern "C" int id11b_dev_score_and_assign_grid(const double* ubis, int64_t m,
                                                        (const int*)(b + L.spos) + n, tol,
                                                        grain_labels, drlv2, labels, npk);
     ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+extern "C" int64_t id11b_grid_refine_workspace_bytes(int64_t m) {
+    if (m < 0) return -1;
+    return (int64_t)al256(sizeof(double) * kLsqF * (size_t)(m > 0 ? m : 1) * score_parts(m));
+}
+
+extern "C" int id11b_dev_refine_grid(double* ubis, int64_t m, const double* gv, int64_t n,
+                                     int32_t nx, int32_t xsub, const void* gridbuf, double tol,
+                                     int iters, int32_t* npk, double* mean, void* ws,
+                                     int64_t ws_bytes, void* stream) {
+    if (m < 0 || n < 0 || iters < 0 || !grid_dims_ok(nx, xsub) || !gridbuf || !ws ||
+        (m > 0 && !ubis) || (n > 0 && !gv) || !(tol >= 0.) || !(tol < 1e3))
+        return ID11B_ERR_ARG;
+    if (((uintptr_t)gridbuf & 255) || ((uintptr_t)ws & 255)) return ID11B_ERR_ALIGN;
+    if (ws_bytes < id11b_grid_refine_workspace_bytes(m)) return ID11B_ERR_SIZE;
+    if (m > INT32_MAX) return ID11B_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (m == 0) return ID11B_OK;
+    const Layout L = layout(n, (int64_t)nx * nx * nx * xsub);
+    const char* b = (const char*)gridbuf;
+    const Header* H = (const Header*)b;
+    const int parts = score_parts(m);
+    const unsigned blocks = (unsigned)((m * parts + kSW - 1) / kSW);
+    double* part = (double*)ws;
+    for (int it = 0; it < iters; it++) {
+        k_refine<<<blocks, kST, 0, st>>>(ubis, m, parts, H, (const int*)(b + L.start),
+                                         (const double*)(b + L.g), tol, part);
+        ID11B_CHECK_LAUNCH();
+        k_refine_finish<<<(unsigned)((m + kGT - 1) / kGT), kGT, 0, st>>>(
+            ubis, m, parts, tol, part, gv, (const int*)(b + L.spec), (const int*)(b + L.spos) + n,
+            npk, mean);
+        ID11B_CHECK_LAUNCH();
+    }
     return ID11B_OK;
 }

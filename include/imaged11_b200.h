@@ -266,6 +266,17 @@ int id11b_dev_score_grid(const double *ubis, int64_t m, const double *gv, int64_
 int id11b_grid_stats(const void *gridbuf, int64_t *nregular, int64_t *nspecial,
                      int64_t *nfallback, int64_t *ntested, void *stream);
 
+/* `iters` rounds of score_and_refine (ImageD11 src/closest.c:267-345) for each
+ * of m UBIs against all n g-vectors through the cell index: the result of
+ * id11b_dev_refine_batch (every pair below tol^2 accumulated in the
+ * reference's FP64 arithmetic; sums in a fixed order), found by lookup.
+ * ws: id11b_grid_refine_workspace_bytes(m), 256-byte aligned. */
+int64_t id11b_grid_refine_workspace_bytes(int64_t m);
+int id11b_dev_refine_grid(double *ubis, int64_t m, const double *gv, int64_t n, int32_t nx,
+                          int32_t xsub, const void *gridbuf, double tol, int iters,
+                          int32_t *npk, double *mean_drlv2, void *ws, int64_t ws_bytes,
+                          void *stream);
+
 /* Batched score_and_assign through the cell index: the result of calling the
  * reference's score_and_assign (ImageD11 src/closest.c:366-397) for grain
  * i = 0 .. m-1 in order, score_and_assign(ubis[i], gv, tol, drlv2, labels,

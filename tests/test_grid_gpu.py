@@ -113,3 +113,23 @@ def test_matches_score_batch(B, scene, cuda):
     a = B.score_grid(ubis, B.GvecGrid(ps.gv), tols).cpu().numpy()
     b = B.score_batch(ubis, B.GvecSet(ps.gv), tols).cpu().numpy()
     assert np.array_equal(a, b)
+
+
+def test_refine_grid_matches_iterated_reference(B, oracle, scene, cuda):
+    from imaged11_b200 import synth
+    ps, _ = scene
+    rng = np.random.default_rng(5)
+    u0 = synth.perturb_ubis(ps.ubis[:50], 0.1, 0.001, rng)
+    u0 = np.concatenate([u0, np.zeros((1, 3, 3))])       # singular: plain scan, unchanged
+    grid = B.GvecGrid(ps.gv)
+    u, npk, mean = B.refine_grid(u0.copy(), grid, 0.05, iters=3)
+    u, npk, mean = u.cpu().numpy(), npk.cpu().numpy(), mean.cpu().numpy()
+    for i in range(len(u0)):
+        uu = u0[i].copy()
+        for _ in range(3):
+            n, m, uu = oracle.score_and_refine(uu, ps.gv, 0.05)
+        assert npk[i] == n
+        assert abs(mean[i] - m) <= 1e-12 * m
+        assert np.abs(u[i] - uu).max() <= 1e-11 * max(np.abs(uu).max(), 1e-300)
+    ub, nb, mb = B.refine_batch(u0.copy(), B.GvecSet(ps.gv), 0.05, iters=3)
+    assert np.array_equal(nb.cpu().numpy(), npk)

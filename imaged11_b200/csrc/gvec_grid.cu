@@ -864,7 +864,7 @@ __global__ void __launch_bounds__(kST, ID11B_GRID_MINB)
 k_assign(const double* __restrict__ ubis, int64_t m, int parts, const Header* __restrict__ Hp,
          const int* __restrict__ start, const double* __restrict__ gs,
          const int* __restrict__ gidx, double tol, const double* __restrict__ drlv2,
-         unsigned long long* __restrict__ best, int* __restrict__ lab) {
+         unsigned long long* __restrict__ best, int* __restrict__ lab, int64_t base) {
     __shared__ unsigned long long s_q[kSW][kQueue];
     __shared__ WarpPlan s_plan[kSW];
     __shared__ Batch s_batch[kSW];
@@ -885,16 +885,18 @@ k_assign(const double* __restrict__ ubis, int64_t m, int parts, const Header* __
         if (PASS == 0)
             atomicMin(best + k, b);
         else if (best[k] == b)
-            atomicMin(lab + k, (int)i);
+            atomicMin(lab + k, (int)(base + i));
     };
     walk(s_plan + w, s_batch + w, s_q[w], ok, part, parts, lane, H, nreg, start, gs, act);
 }
+
+constexpr unsigned long long kNoBest = 0x7fffffffffffffffull;
 
 __global__ void __launch_bounds__(kGT)
 k_assign_init(int64_t n, unsigned long long* __restrict__ best, int* __restrict__ lab) {
     for (int64_t k = (int64_t)blockIdx.x * kGT + threadIdx.x; k < n;
          k += (int64_t)gridDim.x * kGT) {
-        best[k] = ~0ull;
+        best[k] = kNoBest;  // above the bits of every finite drlv2, and positive as int64
         lab[k] = INT_MAX;
     }
 }
@@ -1208,9 +1210,11 @@ extern "C" int id11b_dev_score_and_assign_grid(const double* ubis, int64_t m,
     ID11B_CHECK_LAUNCH();
     const int parts = score_parts(m);
     const unsigned blocks = (unsigned)((m * parts + kSW - 1) / kSW);
-    k_assign<0><<<blocks, kST, 0, st>>>(ubis, m, parts, H, start, gs, gidx, tol, drlv2, best, lab);
+    k_assign<0><<<blocks, kST, 0, st>>>(ubis, m, parts, H, start, gs, gidx, tol, drlv2, best, lab,
+                                        0);
     ID11B_CHECK_LAUNCH();
-    k_assign<1><<<blocks, kST, 0, st>>>(ubis, m, parts, H, start, gs, gidx, tol, drlv2, best, lab);
+    k_assign<1><<<blocks, kST, 0, st>>>(ubis, m, parts, H, start, gs, gidx, tol, drlv2, best, lab,
+                                        0);
     ID11B_CHECK_LAUNCH();
     k_assign_final<<<grid_for(n, kGT), kGT, 0, st>>>(start, ncells, gidx, best, lab, grain_labels,
                                                      m, drlv2, labels, npk);
@@ -1254,5 +1258,74 @@ extern "C" int id11b_dev_refine_grid(double* ubis, int64_t m, const double* gv, 
             npk, mean);
         ID11B_CHECK_LAUNCH();
     }
+    return ID11B_OK;
+}
+
+// The assignment in pieces, for grains sharded over ranks: every rank runs
+// pass -1 (reset) and pass 0 over its share of the grains, the best arrays are
+// reduced with MIN over ranks (int64 view), pass 1 over the share, the lab
+// arrays reduced with MIN (int32), and every rank then applies
+// id11b_dev_assign_grid_final with all m grains (for the g outside the
+// regular range, which follow the reference's sequence of calls).
+extern "C" int id11b_dev_assign_grid_pass(const double* ubis, int64_t m, int64_t index_base,
+                                          int64_t n, int32_t nx, int32_t xsub,
+                                          const void* gridbuf, double tol, const double* drlv2,
+                                          int pass, uint64_t* best, int32_t* lab, void* stream) {
+    if (m < 0 || n < 0 || index_base < 0 || index_base + m > INT32_MAX - 1 ||
+        !grid_dims_ok(nx, xsub) || !gridbuf || !best || !lab || (m > 0 && !ubis) ||
+        (n > 0 && !drlv2) || !(tol >= 0.) || !(tol < 1e3) || pass < -1 || pass > 1)
+        return ID11B_ERR_ARG;
+    if ((uintptr_t)gridbuf & 255) return ID11B_ERR_ALIGN;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (n == 0) return ID11B_OK;
+    if (pass == -1) {
+        k_assign_init<<<grid_for(n, kGT), kGT, 0, st>>>(n, (unsigned long long*)best, lab);
+        ID11B_CHECK_LAUNCH();
+        return ID11B_OK;
+    }
+    if (m == 0) return ID11B_OK;
+    const Layout L = layout(n, (int64_t)nx * nx * nx * xsub);
+    const char* b = (const char*)gridbuf;
+    const int parts = score_parts(m);
+    const unsigned blocks = (unsigned)((m * parts + kSW - 1) / kSW);
+    if (pass == 0)
+        k_assign<0><<<blocks, kST, 0, st>>>(ubis, m, parts, (const Header*)b,
+                                            (const int*)(b + L.start), (const double*)(b + L.g),
+                                            (const int*)(b + L.idx), tol, drlv2,
+                                            (unsigned long long*)best, lab, index_base);
+    else
+        k_assign<1><<<blocks, kST, 0, st>>>(ubis, m, parts, (const Header*)b,
+                                            (const int*)(b + L.start), (const double*)(b + L.g),
+                                            (const int*)(b + L.idx), tol, drlv2,
+                                            (unsigned long long*)best, lab, index_base);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+extern "C" int id11b_dev_assign_grid_final(const double* ubis, int64_t m,
+                                           const int32_t* grain_labels, const double* gv,
+                                           int64_t n, int32_t nx, int32_t xsub,
+                                           const void* gridbuf, double tol, const uint64_t* best,
+                                           const int32_t* lab, double* drlv2, int32_t* labels,
+                                           int32_t* npk, void* stream) {
+    if (m < 0 || n < 0 || !grid_dims_ok(nx, xsub) || !gridbuf || !best || !lab ||
+        (m > 0 && !ubis) || (n > 0 && (!gv || !drlv2 || !labels)) || !(tol >= 0.) ||
+        !(tol < 1e3) || m > INT32_MAX - 1)
+        return ID11B_ERR_ARG;
+    if ((uintptr_t)gridbuf & 255) return ID11B_ERR_ALIGN;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (npk && m > 0) ID11B_CHECK(cudaMemsetAsync(npk, 0, sizeof(int32_t) * (size_t)m, st));
+    if (m == 0 || n == 0) return ID11B_OK;
+    const int64_t ncells = (int64_t)nx * nx * nx * xsub;
+    const Layout L = layout(n, ncells);
+    const char* b = (const char*)gridbuf;
+    k_assign_final<<<grid_for(n, kGT), kGT, 0, st>>>(
+        (const int*)(b + L.start), ncells, (const int*)(b + L.idx),
+        (const unsigned long long*)best, lab, grain_labels, m, drlv2, labels, npk);
+    ID11B_CHECK_LAUNCH();
+    k_assign_special<<<grid_for(n, kGT), kGT, 0, st>>>(ubis, m, gv, (const int*)(b + L.spec),
+                                                       (const int*)(b + L.spos) + n, tol,
+                                                       grain_labels, drlv2, labels, npk);
+    ID11B_CHECK_LAUNCH();
     return ID11B_OK;
 }

@@ -266,6 +266,23 @@ int id11b_dev_score_grid(const double *ubis, int64_t m, const double *gv, int64_
 int id11b_grid_stats(const void *gridbuf, int64_t *nregular, int64_t *nspecial,
                      int64_t *nfallback, int64_t *ntested, void *stream);
 
+/* id11b_dev_score_and_assign_grid in pieces, for grains sharded over ranks
+ * (one process per GPU): each rank runs pass -1 (reset of best (n uint64) and
+ * lab (n int32)) and pass 0 over its share ubis[base : base+m]; best is
+ * reduced with MIN over the ranks as int64; pass 1 over the share; lab reduced
+ * with MIN as int32; then every rank calls id11b_dev_assign_grid_final with
+ * all grains (the g outside the regular range follow the reference's
+ * sequence of calls) and ends with the same drlv2 and labels. */
+int id11b_dev_assign_grid_pass(const double *ubis, int64_t m, int64_t index_base, int64_t n,
+                               int32_t nx, int32_t xsub, const void *gridbuf, double tol,
+                               const double *drlv2, int pass, uint64_t *best, int32_t *lab,
+                               void *stream);
+int id11b_dev_assign_grid_final(const double *ubis, int64_t m, const int32_t *grain_labels,
+                                const double *gv, int64_t n, int32_t nx, int32_t xsub,
+                                const void *gridbuf, double tol, const uint64_t *best,
+                                const int32_t *lab, double *drlv2, int32_t *labels,
+                                int32_t *npk, void *stream);
+
 /* `iters` rounds of score_and_refine (ImageD11 src/closest.c:267-345) for each
  * of m UBIs against all n g-vectors through the cell index: the result of
  * id11b_dev_refine_batch (every pair below tol^2 accumulated in the

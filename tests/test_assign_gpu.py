@@ -88,3 +88,32 @@ def test_bad_grain_labels(scene, cuda):
     with pytest.raises(ValueError):
         batch.score_and_assign_grid(ubis[:3], batch.GvecGrid(ps.gv), 0.1, d, lab,
                                     grain_labels=[3, 2, 5])
+
+
+def test_sharded_passes_on_one_gpu(scene, oracle, cuda):
+    """The sharded driver with the CUDA passes (world 1 over gloo; the
+    multi-rank exchange itself is covered by tests/test_multirank.py)."""
+    import datetime
+    import socket
+    import torch
+    import torch.distributed as dist
+    from imaged11_b200 import batch, shard
+    ps, ubis = scene
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=0,
+                            world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        grid = batch.GvecGrid(ps.gv)
+        n = len(ps.gv)
+        d = torch.full((n,), 2.0, dtype=torch.float64, device=cuda)
+        lab = torch.full((n,), -1, dtype=torch.int32, device=cuda)
+        shard.score_and_assign_sharded(ubis, 0.1, d, lab, shard.CudaAssignPasses(grid),
+                                       device="cpu")
+        d2 = torch.full((n,), 2.0, dtype=torch.float64, device=cuda)
+        lab2 = torch.full((n,), -1, dtype=torch.int32, device=cuda)
+        batch.score_and_assign_grid(ubis, grid, 0.1, d2, lab2)
+        assert torch.equal(lab, lab2) and torch.equal(d, d2)
+    finally:
+        dist.destroy_process_group()

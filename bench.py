@@ -715,9 +715,13 @@ def run_ours(args, rank, world, local_rank):
                                 cpu=(world == 1))
     adj = adjoint_measure(torch, dev, steps=max(3, args.steps))
     trans = translations_measure(torch, dev, steps=max(3, args.steps), cpu=(world == 1))
-    # the same scoring through the reciprocal-space cell index (exact FP64 lookups)
+    # the same scoring through the reciprocal-space cell index (exact FP64 lookups),
+    # index shape from the autotuner (untimed setup)
+    grid_shape, grid_table = tune.tune_grid(ubis_d, gs.gv, TOLS, reps=2)
     cell = grid_measure(torch, dev, ps, ubis, steps=max(3, args.steps), flush=flush,
                         check_counts=counts)
+    cell["tuned_shape"] = {"cell_factor": grid_shape[0], "xsub": grid_shape[1]}
+    cell["tuning_ms"] = {"%g,%d" % t: round(ms, 3) for t, ms in grid_table}
     cell["ratio_vs_fp32_screening"] = cell["value"] / value
     cell["ratio_vs_plain_fp64_all_tols"] = cell["value"] / rate64f
 

@@ -154,6 +154,13 @@ class GvecGrid:
         self.gmax, self.rmax = float(b[0]), float(b[1])
         nx = ctypes.c_int32(0)
         cs = ctypes.c_double(0.)
+        if cell is None and xsub is None:  # a shape tune.tune_grid found for this size
+            from . import tune
+            shape = tune.grid_shape(self.n)
+            if shape:
+                check(lib.id11b_grid_plan(self.gmax, self.n, 0., ctypes.addressof(nx),
+                                          ctypes.addressof(cs)), "grid_plan")
+                cell, xsub = cs.value * shape[0], int(shape[1])
         check(lib.id11b_grid_plan(self.gmax, self.n, float(cell or 0.), ctypes.addressof(nx),
                                   ctypes.addressof(cs)), "grid_plan")
         self.nx, self.cs = nx.value, cs.value

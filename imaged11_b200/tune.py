@@ -10,6 +10,8 @@ candidates with CUDA events on the caller's own inputs:
   into, i.e. how many 1,024-vector shared-memory tiles a CTA streams).
   Counts are identical for every tile shape, so tuning needs no reference.
 * GrainSet CTA size for the persistent per-grain refinement (32..256).
+* the cell index's shape (y/z cell side relative to about one g per cell, and
+  how many times finer x is cut), timed with score_grid.
 
 Results are cached per (device, shape bucket): m and n rounded up to powers of
 two.  ``save``/``load`` persist the cache as JSON; setting
@@ -145,6 +147,44 @@ def refine_threads(ngrains, peaks):
     if not _cache:
         return None
     return _cache.get(refine_key(ngrains, peaks))
+
+
+def grid_key(n):
+    return "grid|%s|%d" % (_device_name(), _bucket(n))
+
+
+def tune_grid(ubis, gv, tols, cell_factors=(0.8, 1.0, 1.25), xsubs=(1, 2, 4, 8), reps=2):
+    """Time score_grid on these inputs for cell-index shapes: y/z cell side =
+    factor x the default (about one g per cell of the bounding cube) and x cut
+    xsub times finer; cache the fastest per g-count bucket (GvecGrid uses it
+    when built without explicit shape) and return ((factor, xsub), table)."""
+    from . import batch
+    torch = _torch()
+    g = batch._dev(gv, torch.float64).reshape(-1, 3)
+    u = batch._dev(ubis, torch.float64).reshape(-1, 9)
+    base = batch.GvecGrid(g, xsub=1)
+    out = torch.empty((u.shape[0], len(batch._tols(tols))), dtype=torch.int32, device=g.device)
+    table = []
+    for f in cell_factors:
+        for xs in xsubs:
+            grid = batch.GvecGrid(g, cell=base.cs * f, xsub=xs)
+            if grid.xsub != xs:
+                continue  # over the cell budget
+            ms = _time(lambda: batch.score_grid(u, grid, tols, out=out), reps)
+            table.append(((f, xs), ms))
+            del grid
+    best = min(table, key=lambda x: x[1])[0]
+    _cache[grid_key(g.shape[0])] = list(best)
+    _autosave()
+    return best, table
+
+
+def grid_shape(n):
+    """The tuned (cell factor, xsub) for this many g-vectors, or None."""
+    if not _cache:
+        return None
+    t = _cache.get(grid_key(n))
+    return tuple(t) if t else None
 
 
 def save(path):

@@ -90,3 +90,18 @@ def test_refine_tuner(tune, oracle, cuda):
     scale = np.abs(ref_u).reshape(ng, -1).max(1)
     err = np.abs(u.cpu().numpy() - ref_u).reshape(ng, -1).max(1)
     assert np.all(err <= 1e-11 * scale)
+
+
+@pytest.mark.gpu
+def test_grid_tuner(tune, oracle, cuda):
+    from imaged11_b200 import batch, synth
+    ps = synth.simulate(60, "Al", gmax=1.2, seed=55, noise_frac=0.1)
+    rng = np.random.default_rng(56)
+    ubis = synth.trial_ubis(ps.ubis, 500, 0.1, 0.5, rng)
+    tols = [0.05, 0.1]
+    best, table = tune.tune_grid(ubis, ps.gv, tols, reps=1)
+    assert best in [t for t, _ in table]
+    grid = batch.GvecGrid(ps.gv)                      # picks the tuned shape
+    assert grid.xsub == best[1]
+    ref = oracle.score_many(ubis, ps.gv, tols)
+    assert np.array_equal(batch.score_grid(ubis, grid, tols).cpu().numpy(), ref)

@@ -709,6 +709,23 @@ def run_ours(args, rank, world, local_rank):
     # compute_gv (HBM-bound FP64 streaming kernel), 10M peaks
     gv_gbs, gv_ms = compute_gv_measure(torch, ps, dev, 10_000_000, max(3, args.steps), flush)
     hbm_peak, hbm_kind = measured_hbm_peak()
+    gv_cpu = None
+    if world == 1:  # the reference's OpenMP compute_gv on the host cores, 2M peaks
+        from oracle import oracle as orcm
+        ref = orcm.Reference() if orcm.have_reference() else orcm.Oracle()
+        reps = -(-2_000_000 // len(ps.xyz))
+        xh = np.ascontiguousarray(np.tile(ps.xyz, (reps, 1))[:2_000_000])
+        oh = np.ascontiguousarray(np.tile(ps.omega, reps)[:2_000_000])
+        geo = ps.geo
+        ref.compute_gv(xh[:1000], oh[:1000], geo["omegasign"], geo["wavelength"], 0., 0.,
+                       np.zeros(3))
+        t0 = time.perf_counter()
+        ref.compute_gv(xh, oh, geo["omegasign"], geo["wavelength"], 0., 0., np.zeros(3))
+        dt = time.perf_counter() - t0
+        gv_cpu = {"value": 56.0 * len(oh) / dt / 1e9, "unit": "GB/s",
+                  "cores": ref.max_threads(),
+                  "kind": "reference" if isinstance(ref, orcm.Reference) else "port",
+                  "sample": "2,000,000 peaks (%.3f s)" % dt}
 
     # uneven per-grain refinement (persistent kernel in a CUDA graph)
     refine = refine_csr_measure(torch, dev, steps=max(3, args.steps), flush=flush,
@@ -775,6 +792,7 @@ def run_ours(args, rank, world, local_rank):
         "adjoint": adj,
         "translations": trans,
         "compute_gv": {"peaks": 10_000_000, "ms": gv_ms, "achieved_gbs": gv_gbs,
+                       "cpu_baseline": gv_cpu,
                        "peak_gbs": hbm_peak, "peak_kind": hbm_kind,
                        "frac": gv_gbs / hbm_peak, "bytes_per_peak": 56},
         "recheck": {"fp64_pairs": nrecheck, "fraction": nrecheck / (m * n),

@@ -434,6 +434,11 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5):
                    npk_median=int(grains.npk.median().item()))
 
     run([torch.cuda.Event(enable_timing=True) for _ in range(6)])   # warm-up (module loads)
+    # index shape for this peak set from the autotuner, on a tenth of the trials
+    # (untimed setup; the counts do not depend on it)
+    from imaged11_b200 import tune
+    shape, _ = tune.tune_grid(ub_d[::10], gv, [tol], cell_factors=(1.0, 1.25, 1.6),
+                              xsubs=(1, 2, 4), reps=1)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
     run(ev)
     names = ["compute_xlylzl+compute_gv", "cell_index+score_grid", "score_and_assign",
@@ -455,6 +460,7 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5):
             "stage_ms": stages, "pairs": pairs, "device_ms": device_ms,
             "value": pairs / (device_ms * 1e-3), "unit": "pairs/s",
             "assigned_peaks": out["assigned"], "peaks_per_grain_median": out["npk_median"],
+            "index_shape": {"cell_factor": shape[0], "xsub": shape[1]},
             "score_batch_fp32_ms": e0.elapsed_time(e1),
             "score_grid_counts_equal_fp32": bool(torch.equal(c32, cbuf)),
             "trial_counts_median_max": [int(cbuf[:, 0].median().item()),

@@ -39,7 +39,7 @@ L2_FLUSH_BYTES = 256 << 20
 
 
 def measured_hbm_peak():
-    """Measured HBM copy bandwidth for this GPU pool (GB/s), else the fallback."""
+    """Measured HBM copy bandwidth of this GPU model (GB/s), else the fallback."""
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
         with open(path) as f:

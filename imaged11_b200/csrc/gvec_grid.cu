@@ -4,8 +4,9 @@
 // against a UBI.  A g-vector is counted iff |UBI.g - round(UBI.g)|^2 < tol^2,
 // i.e. iff it lies inside the ellipsoid of radius tol (in hkl units) around
 // UB.hkl for hkl = round(UBI.g), UB = UBI^-1.  This file bins the g-vectors
-// into a uniform grid of cubic cells (x fastest, so a row of cells along x is
-// one contiguous range of the cell-sorted g), then for each UBI enumerates
+// into a uniform grid of cells (square in y and z, x cut finer; x fastest, so
+// a row of cells along x is one contiguous range of the cell-sorted g), then
+// for each UBI enumerates
 // the integer hkl whose ellipsoid can reach the data and tests only the g in
 // the cells overlapping a conservative bounding box of that ellipsoid.  Every
 // tested pair is evaluated with the reference's exact FP64 arithmetic
@@ -296,7 +297,6 @@ struct Plan {
     double w[3];       // box half-widths
     int64_t lo[3];     // hkl box
     int64_t nh[3];
-    int64_t total;     // hkl in the box
     bool ok;           // false: plain scan of every regular g
 };
 
@@ -345,7 +345,6 @@ __device__ __forceinline__ Plan make_plan(const double u[9], double tmax, const 
         ok = ok && isfinite(P.w[r]);
     }
     ok = ok && total <= (double)nreg;  // more candidate hkl than g: the plain scan is cheaper
-    P.total = ok ? P.nh[0] * P.nh[1] * P.nh[2] : 0;
     P.ok = ok;
     return P;
 }

@@ -30,6 +30,8 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 TOLS = [0.02, 0.05, 0.1]
+# DRAM bytes of one screening-kernel launch on this workload's g-vectors (ncu capture)
+K_BATCH_DRAM_BYTES = 19.8e6
 N_GRAINS = 2000
 GMAX = 1.5
 N_UBI = 20000
@@ -786,7 +788,12 @@ def run_ours(args, rank, world, local_rank):
                 "h2d_bytes_per_step": int(ps.gv.nbytes + ubis.nbytes),
                 "d2h_bytes_per_step": int(m * T * 4)},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                     "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "traffic": K_BATCH_DRAM_BYTES,
+                     "traffic_note": "dram__bytes_read.sum + write.sum of one k_batch launch "
+                                     "captured with 2,048 UBIs (profiles/); the g tiles come "
+                                     "from L2 after their first read, so the DRAM bytes do not "
+                                     "grow with the UBI count",
                      "kernel": "k_batch<%d,3,score>" % tile[0],
                      "peak_note": "CUDA-core FP32 = SMs x 128 x 2 x median SM clock under load; "
                                   "%d FLOP per (UBI,g) evaluation" % FLOP_PER_EVAL},

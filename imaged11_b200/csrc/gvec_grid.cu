@@ -709,13 +709,49 @@ k_score(const double* __restrict__ ubis, int64_t m, int parts, Header* __restric
     if (lane == 0 && tt) atomicAdd(&Hp->ntested, (unsigned long long)tt);
 }
 
-// One thread per UBI: CTA-part partials in a fixed order, then the g-vectors
-// outside the regular range, one by one in list order.
+// The g-vectors outside the regular range, one warp per UBI: lanes stride the
+// list, fixed-tree warp sums, one slot per UBI and tolerance.
 __global__ void __launch_bounds__(kGT)
-k_score_finish(const double* __restrict__ ubis, int64_t m, int parts, int ntol, Tols tols,
-               const int* __restrict__ pcnt, const double* __restrict__ psum,
-               const double* __restrict__ gv, const int* __restrict__ special,
-               const int* __restrict__ nspecial, int* __restrict__ counts,
+k_score_special(const double* __restrict__ ubis, int64_t m, int ntol, Tols tols,
+                const double* __restrict__ gv, const int* __restrict__ special,
+                const int* __restrict__ nspecial, int* __restrict__ scnt,
+                double* __restrict__ ssum) {
+    const int64_t i = ((int64_t)blockIdx.x * kGT + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= m) return;  // uniform per warp
+    int c[ID11B_MAX_TOLS] = {0, 0, 0, 0};
+    double sm[ID11B_MAX_TOLS] = {0., 0., 0., 0.};
+    const int ns = *nspecial;
+    if (ns) {
+        double u[9];
+        for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
+        for (int q = lane; q < ns; q += 32) {
+            const int64_t k = special[q];
+            double ih[3];
+            const double v = drlv2_exact(u, gv[3 * k], gv[3 * k + 1], gv[3 * k + 2], ih);
+            for (int j = 0; j < ntol; j++)
+                if (v < tols.t[j] * tols.t[j]) {
+                    c[j]++;
+                    sm[j] += v;
+                }
+        }
+    }
+    for (int j = 0; j < ntol; j++) {
+        const int cs = warp_sum(c[j]);
+        const double ss = warp_sum(sm[j]);
+        if (lane == 0) {
+            scnt[i * ntol + j] = cs;
+            ssum[i * ntol + j] = ss;
+        }
+    }
+}
+
+// One thread per UBI: CTA-part partials in a fixed order, then the slot of
+// the g-vectors outside the regular range.
+__global__ void __launch_bounds__(kGT)
+k_score_finish(int64_t m, int parts, int ntol, const int* __restrict__ pcnt,
+               const double* __restrict__ psum, const int* __restrict__ scnt,
+               const double* __restrict__ ssum, int* __restrict__ counts,
                double* __restrict__ sums) {
     const int64_t i = (int64_t)blockIdx.x * kGT + threadIdx.x;
     if (i >= m) return;
@@ -726,24 +762,9 @@ k_score_finish(const double* __restrict__ ubis, int64_t m, int parts, int ntol, 
             c[j] += pcnt[(i * parts + p) * ntol + j];
             s[j] += psum[(i * parts + p) * ntol + j];
         }
-    const int ns = *nspecial;
-    if (ns) {
-        double u[9];
-        for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
-        for (int q = 0; q < ns; q++) {
-            const int64_t k = special[q];
-            double ih[3];
-            const double v = drlv2_exact(u, gv[3 * k], gv[3 * k + 1], gv[3 * k + 2], ih);
-            for (int j = 0; j < ntol; j++)
-                if (v < tols.t[j] * tols.t[j]) {
-                    c[j]++;
-                    s[j] += v;
-                }
-        }
-    }
     for (int j = 0; j < ntol; j++) {
-        counts[i * ntol + j] = c[j];
-        if (sums) sums[i * ntol + j] = s[j];
+        counts[i * ntol + j] = c[j] + scnt[i * ntol + j];
+        if (sums) sums[i * ntol + j] = s[j] + ssum[i * ntol + j];
     }
 }
 
@@ -804,13 +825,43 @@ k_refine(const double* __restrict__ ubis, int64_t m, int parts, const Header* __
     }
 }
 
-// One thread per UBI: partials in part order, then the g outside the regular
-// range in list order, then the reference's update; n and mean drlv2 of the
-// UBI as it was on entry.
+// The g-vectors outside the regular range, one warp per UBI: normal-equation
+// terms of the pairs below tol^2 (lanes stride the list, fixed-tree sums).
 __global__ void __launch_bounds__(kGT)
-k_refine_finish(double* __restrict__ ubis, int64_t m, int parts, double tol,
-                const double* __restrict__ part_in, const double* __restrict__ gv,
-                const int* __restrict__ special, const int* __restrict__ nspecial,
+k_refine_special(const double* __restrict__ ubis, int64_t m, double tol,
+                 const double* __restrict__ gv, const int* __restrict__ special,
+                 const int* __restrict__ nspecial, double* __restrict__ spart) {
+    __shared__ double s_lsq[kGT / 32][kLsqF * 32];
+    const int64_t i = ((int64_t)blockIdx.x * kGT + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= m) return;  // uniform per warp
+    double* acc = s_lsq[threadIdx.x >> 5] + lane;
+    for (int f = 0; f < kLsqF; f++) acc[f * 32] = 0.;
+    const int ns = *nspecial;
+    if (ns) {
+        double u[9];
+        for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
+        for (int q = lane; q < ns; q += 32) {
+            const int64_t k = special[q];
+            double ih[3];
+            const double g[3] = {gv[3 * k], gv[3 * k + 1], gv[3 * k + 2]};
+            const double sv = drlv2_exact(u, g[0], g[1], g[2], ih);
+            if (sv < tol * tol) lsq_add(acc, sv, g, ih);
+        }
+    }
+    __syncwarp();
+    for (int f = 0; f < kLsqF; f++) {
+        const double v = warp_sum(acc[f * 32]);
+        if (lane == 0) spart[i * kLsqF + f] = v;
+    }
+}
+
+// One thread per UBI: partials in part order, then the slot of the g outside
+// the regular range, then the reference's update; n and mean drlv2 of the UBI
+// as it was on entry.
+__global__ void __launch_bounds__(kGT)
+k_refine_finish(double* __restrict__ ubis, int64_t m, int parts,
+                const double* __restrict__ part_in, const double* __restrict__ spart,
                 int* __restrict__ npk, double* __restrict__ mean) {
     const int64_t i = (int64_t)blockIdx.x * kGT + threadIdx.x;
     if (i >= m) return;
@@ -818,27 +869,9 @@ k_refine_finish(double* __restrict__ ubis, int64_t m, int parts, double tol,
     for (int f = 0; f < kLsqF; f++) t[f] = 0.;
     for (int p = 0; p < parts; p++)
         for (int f = 0; f < kLsqF; f++) t[f] += part_in[(i * parts + p) * kLsqF + f];
+    for (int f = 0; f < kLsqF; f++) t[f] += spart[i * kLsqF + f];
     double u[9];
     for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
-    const int ns = *nspecial;
-    for (int q = 0; q < ns; q++) {
-        const int64_t k = special[q];
-        double ih[3];
-        const double g[3] = {gv[3 * k], gv[3 * k + 1], gv[3 * k + 2]};
-        const double s = drlv2_exact(u, g[0], g[1], g[2], ih);
-        if (s < tol * tol) {
-            for (int a = 0; a < 3; a++)
-                for (int b = 0; b < 3; b++) t[3 * a + b] = dadd(t[3 * a + b], dmul(ih[b], g[a]));
-            t[9] = dadd(t[9], dmul(ih[0], ih[0]));
-            t[10] = dadd(t[10], dmul(ih[1], ih[0]));
-            t[11] = dadd(t[11], dmul(ih[2], ih[0]));
-            t[12] = dadd(t[12], dmul(ih[1], ih[1]));
-            t[13] = dadd(t[13], dmul(ih[2], ih[1]));
-            t[14] = dadd(t[14], dmul(ih[2], ih[2]));
-            t[15] = dadd(t[15], s);
-            t[16] += 1.0;
-        }
-    }
     double R[9], Hm[9];
     for (int f = 0; f < 9; f++) R[f] = t[f];
     Hm[0] = t[9];  Hm[1] = t[10]; Hm[2] = t[11];
@@ -1105,9 +1138,12 @@ extern "C" int id11b_dev_build_grid(const double* gv, int64_t n, float gmax, flo
     return ID11B_OK;
 }
 
+// partials: (m * parts + m) x ntol ints, then the same doubles (the last m x
+// ntol of each: the g outside the regular range)
 extern "C" int64_t id11b_grid_score_workspace_bytes(int64_t m, int ntol) {
     if (m < 0 || ntol < 1 || ntol > ID11B_MAX_TOLS) return -1;
-    const int64_t items = (m > 0 ? m : 1) * score_parts(m) * ntol;
+    const int64_t mm = m > 0 ? m : 1;
+    const int64_t items = (mm * score_parts(m) + mm) * ntol;
     return (int64_t)(al256(sizeof(int) * (size_t)items) + al256(sizeof(double) * (size_t)items));
 }
 
@@ -1133,9 +1169,11 @@ extern "C" int id11b_dev_score_grid(const double* ubis, int64_t m, const double*
     ID11B_CHECK(cudaMemsetAsync(&H->nfallback, 0, 2 * sizeof(unsigned long long), st));
     if (m == 0) return ID11B_OK;
     const int parts = score_parts(m);
-    const int64_t items = m * parts * ntol;
+    const int64_t items = (m * parts + m) * ntol;
     int* pcnt = (int*)ws;
     double* psum = (double*)((char*)ws + al256(sizeof(int) * (size_t)items));
+    int* scnt = pcnt + m * parts * ntol;
+    double* ssum = psum + m * parts * ntol;
     const int64_t warps = m * parts;
     const unsigned blocks = (unsigned)((warps + kSW - 1) / kSW);
     const int* start = (const int*)(b + L.start);
@@ -1147,9 +1185,12 @@ extern "C" int id11b_dev_score_grid(const double* ubis, int64_t m, const double*
         default: k_score<4><<<blocks, kST, 0, st>>>(ubis, m, parts, H, start, gs, T, pcnt, psum); break;
     }
     ID11B_CHECK_LAUNCH();
-    k_score_finish<<<(unsigned)((m + kGT - 1) / kGT), kGT, 0, st>>>(
-        ubis, m, parts, ntol, T, pcnt, psum, gv, (const int*)(b + L.spec),
-        (const int*)(b + L.spos) + n, counts, sums);
+    k_score_special<<<(unsigned)((m * 32 + kGT - 1) / kGT), kGT, 0, st>>>(
+        ubis, m, ntol, T, gv, (const int*)(b + L.spec), (const int*)(b + L.spos) + n, scnt,
+        ssum);
+    ID11B_CHECK_LAUNCH();
+    k_score_finish<<<(unsigned)((m + kGT - 1) / kGT), kGT, 0, st>>>(m, parts, ntol, pcnt, psum,
+                                                                    scnt, ssum, counts, sums);
     ID11B_CHECK_LAUNCH();
     return ID11B_OK;
 }
@@ -1225,9 +1266,12 @@ extern "C" int id11b_dev_score_and_assign_grid(const double* ubis, int64_t m,
     return ID11B_OK;
 }
 
+// partials: m * parts + m slots of 17 doubles (the last m: the g outside the
+// regular range)
 extern "C" int64_t id11b_grid_refine_workspace_bytes(int64_t m) {
     if (m < 0) return -1;
-    return (int64_t)al256(sizeof(double) * kLsqF * (size_t)(m > 0 ? m : 1) * score_parts(m));
+    const size_t mm = (size_t)(m > 0 ? m : 1);
+    return (int64_t)al256(sizeof(double) * kLsqF * (mm * score_parts(m) + mm));
 }
 
 extern "C" int id11b_dev_refine_grid(double* ubis, int64_t m, const double* gv, int64_t n,
@@ -1252,9 +1296,12 @@ extern "C" int id11b_dev_refine_grid(double* ubis, int64_t m, const double* gv, 
         k_refine<<<blocks, kST, 0, st>>>(ubis, m, parts, H, (const int*)(b + L.start),
                                          (const double*)(b + L.g), tol, part);
         ID11B_CHECK_LAUNCH();
-        k_refine_finish<<<(unsigned)((m + kGT - 1) / kGT), kGT, 0, st>>>(
-            ubis, m, parts, tol, part, gv, (const int*)(b + L.spec), (const int*)(b + L.spos) + n,
-            npk, mean);
+        double* spart = part + m * parts * kLsqF;
+        k_refine_special<<<(unsigned)((m * 32 + kGT - 1) / kGT), kGT, 0, st>>>(
+            ubis, m, tol, gv, (const int*)(b + L.spec), (const int*)(b + L.spos) + n, spart);
+        ID11B_CHECK_LAUNCH();
+        k_refine_finish<<<(unsigned)((m + kGT - 1) / kGT), kGT, 0, st>>>(ubis, m, parts, part,
+                                                                         spart, npk, mean);
         ID11B_CHECK_LAUNCH();
     }
     return ID11B_OK;

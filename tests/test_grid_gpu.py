@@ -133,3 +133,20 @@ def test_refine_grid_matches_iterated_reference(B, oracle, scene, cuda):
         assert np.abs(u[i] - uu).max() <= 1e-11 * max(np.abs(uu).max(), 1e-300)
     ub, nb, mb = B.refine_batch(u0.copy(), B.GvecSet(ps.gv), 0.05, iters=3)
     assert np.array_equal(nb.cpu().numpy(), npk)
+
+
+def test_refine_grid_special_g(B, golden, oracle, cuda):
+    d = golden["scoring"]
+    gv = d["adv_gv"]
+    u0 = np.concatenate([d["adv_ubi"][None], d["sc_ubis"][:5]])
+    grid = B.GvecGrid(gv)
+    assert grid.stats()["special"] > 0
+    u, npk, mean = B.refine_grid(u0.copy(), grid, 0.1, iters=2)
+    u, npk, mean = u.cpu().numpy(), npk.cpu().numpy(), mean.cpu().numpy()
+    for i in range(len(u0)):
+        uu = u0[i].copy()
+        for _ in range(2):
+            n, m, uu = oracle.score_and_refine(uu, gv, 0.1)
+        assert npk[i] == n
+        assert abs(mean[i] - m) <= 1e-12 * m
+        assert np.abs(u[i] - uu).max() <= 1e-11 * np.abs(uu).max()

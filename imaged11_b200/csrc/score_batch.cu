@@ -46,6 +46,12 @@ constexpr int kBT = 256;            // threads per CTA
 #define ID11B_SCORE_UBIS_PER_THREAD 4
 #endif
 constexpr int kScoreR = ID11B_SCORE_UBIS_PER_THREAD;
+// g-vectors per unrolled step of the screening loop (20,000 UBIs x 1.1M g on
+// B200, autotuned tiles: 17.97 / 17.33 / 16.86-17.03 / 27.6 ms at 1 / 2 / 4 / 8)
+#ifndef ID11B_SCORE_UNROLL
+#define ID11B_SCORE_UNROLL 4
+#endif
+constexpr int kScoreUnroll = ID11B_SCORE_UNROLL;
 // resident CTAs per SM the screening kernel is compiled for (register budget)
 __host__ __device__ constexpr int score_ctas_per_sm(int r) { return r <= 2 ? 4 : r <= 4 ? 3 : 2; }
 constexpr int kTile = 1024;         // g per TMA tile (16 KB of float4)
@@ -326,7 +332,7 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
         }
         const int64_t a = k0 + (int64_t)t * kTile;
         const int cntg = (int)min((int64_t)kTile, k1 - a);
-#pragma unroll 2
+#pragma unroll kScoreUnroll
         for (int k = 0; k < cntg; k++) {
             const float4 g = s_g[buf][k];
             const uint64_t gx = pk2(g.x, g.x), gy = pk2(g.y, g.y), gz = pk2(g.z, g.z);

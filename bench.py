@@ -134,9 +134,26 @@ def grid_measure(torch, dev, ps, ubis, steps=5, flush=None, check_counts=None, c
     t_rb = float(np.mean(cuda_time_ms(
         torch, lambda: batch.refine_batch(ubis_d.clone(), gs, 0.05, workspace=rws), steps,
         flush)))
+    # errors of one indexed round against the reference arithmetic, 32 UBIs
+    from oracle import oracle as orcm
+    orc = orcm.Reference() if orcm.have_reference() else orcm.Oracle()
+    ug, ng_, mg = batch.refine_grid(ubis_d[:32].clone(), grid, 0.05)
+    ug, ng_, mg = ug.cpu().numpy().reshape(-1, 9), ng_.cpu().numpy(), mg.cpu().numpy()
+    e_u = e_m = 0.0
+    same_n = True
+    for q in range(32):
+        rn, rmean, ru = orc.score_and_refine(ubis[q], ps.gv, 0.05)
+        same_n &= int(rn) == int(ng_[q])
+        sc = max(np.abs(ru).max(), 1e-300)
+        e_u = max(e_u, float(np.abs(ug[q] - np.asarray(ru).reshape(9)).max() / sc))
+        if rmean:
+            e_m = max(e_m, abs(mg[q] - rmean) / rmean)
     return {"ms": ms, "value": m * n * T / (ms * 1e-3), "unit": "pairs/s",
             "refine": {"ubis": m, "tol": 0.05, "grid_ms": t_rg, "batch_fp32_ms": t_rb,
-                       "value": m * n / (t_rg * 1e-3), "batch_value": m * n / (t_rb * 1e-3)},
+                       "value": m * n / (t_rg * 1e-3), "batch_value": m * n / (t_rb * 1e-3),
+                       "vs_reference_32_ubis": {"npk_identical": bool(same_n),
+                                                "ubi_max_rel_err": e_u,
+                                                "mean_drlv2_max_rel_err": float(e_m)}},
             "assign": {"ubis": m, "tol": 0.05, "ms": t_asg, "value": m * n / (t_asg * 1e-3),
                        "sequential_plain_fp64_value": k * n / (t_seq * 1e-3),
                        "sequential_ubis": k, "identical_to_sequential": same_assign},
@@ -240,8 +257,24 @@ def refine_csr_measure(torch, dev, iters=5, tol=0.05, steps=5, flush=None, cpu=T
         from oracle import oracle as orc
         lib = orc.Reference() if orc.have_reference() else orc.Oracle()
         t0 = time.perf_counter()
-        lib.refine_csr(u0, gv, off, tol, iters)
+        ref_u, ref_n, ref_m = lib.refine_csr(u0, gv, off, tol, iters)
         dt = time.perf_counter() - t0
+        # the graph's result against the reference's: the max error of every UBI
+        # element (relative to the grain's largest element) and of mean drlv2
+        reset()
+        graph.replay()
+        torch.cuda.synchronize()
+        gu = gs.ubis.cpu().numpy().reshape(-1, 9)
+        ru = np.asarray(ref_u).reshape(-1, 9)
+        scale = np.abs(ru).max(1, keepdims=True)
+        scale[scale == 0] = 1.0
+        gm, rm = gs.mean.cpu().numpy(), np.asarray(ref_m)
+        nz = rm != 0
+        out["vs_reference"] = {
+            "npk_identical": bool(np.array_equal(gs.npk.cpu().numpy(), np.asarray(ref_n))),
+            "ubi_max_rel_err": float((np.abs(gu - ru) / scale).max()),
+            "mean_drlv2_max_rel_err": float((np.abs(gm[nz] - rm[nz]) / rm[nz]).max())
+            if nz.any() else 0.0}
         out["cpu_baseline"] = {"value": pairs / dt, "unit": "pairs/s",
                                "cores": lib.max_threads(),
                                "kind": "reference" if isinstance(lib, orc.Reference) else "port",

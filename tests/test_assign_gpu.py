@@ -117,3 +117,27 @@ def test_sharded_passes_on_one_gpu(scene, oracle, cuda):
         assert torch.equal(lab, lab2) and torch.equal(d, d2)
     finally:
         dist.destroy_process_group()
+
+
+def test_random_sweep(oracle, cuda):
+    from imaged11_b200 import batch
+    rng = np.random.default_rng(79)
+    for trial in range(10):
+        n = int(rng.integers(1, 3000))
+        gv = rng.normal(size=(n, 3)) * rng.uniform(0.3, 1.5)
+        m = int(rng.integers(1, 60))
+        ubis = np.empty((m, 3, 3))
+        for i in range(m):
+            q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            ubis[i] = np.diag(rng.uniform(2.0, 10.0, 3)) @ q.T
+        ubis[m // 2] = ubis[0]                      # a tie
+        tol = float(rng.uniform(0.01, 0.4))
+        d0 = rng.uniform(0.0, 0.2, n)
+        l0 = rng.choice(np.arange(-1, m + 3), n).astype(np.int32)
+        d, lab = d0.copy(), l0.copy()
+        for i, u in enumerate(ubis):
+            _, d, lab = oracle.score_and_assign(u, gv, tol, d, lab, i)
+        dd, ll = d0.copy(), l0.copy()
+        batch.score_and_assign_grid(ubis, batch.GvecGrid(gv), tol, dd, ll)
+        assert np.array_equal(ll, lab), trial
+        assert np.array_equal(dd, d), trial

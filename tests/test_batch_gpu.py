@@ -131,3 +131,22 @@ def test_refine_batch_matches_iterated_reference(B, oracle, scene, cuda):
         assert npk[i] == n
         assert abs(mean[i] - m) <= 1e-12 * m
         assert np.abs(u[i] - uu).max() <= UBI_RTOL * np.abs(uu).max()
+
+
+def test_random_sweep(B, oracle, cuda):
+    """Random cells, orientations, g clouds and tolerances (g on rounding
+    half-points included) against the oracle, through the FP32 screening."""
+    rng = np.random.default_rng(78)
+    for trial in range(24):
+        n = int(rng.integers(1, 6000))
+        gv = rng.normal(size=(n, 3)) * rng.uniform(0.2, 2.0)
+        m = int(rng.integers(1, 700))
+        ubis = np.empty((m, 3, 3))
+        for i in range(m):
+            q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            ubis[i] = np.diag(rng.uniform(1.5, 12.0, 3)) @ q.T
+        if trial % 3 == 1:
+            gv[: n // 3] = np.linalg.solve(ubis[0], (rng.integers(-5, 5, (n // 3, 3)) + 0.5).T).T
+        tols = sorted(rng.uniform(0.001, 0.6, int(rng.integers(1, 5))).tolist())
+        c = B.score_batch(ubis, B.GvecSet(gv), tols).cpu().numpy()
+        assert np.array_equal(c, oracle.score_many(ubis, gv, tols)), trial

@@ -150,3 +150,27 @@ def test_refine_grid_special_g(B, golden, oracle, cuda):
         assert npk[i] == n
         assert abs(mean[i] - m) <= 1e-12 * m
         assert np.abs(u[i] - uu).max() <= 1e-11 * np.abs(uu).max()
+
+
+def test_random_sweep(B, oracle, cuda):
+    """Random cells, orientations, g clouds and tolerances (including ones above
+    0.5 and g on the rounding half-points) against the oracle."""
+    rng = np.random.default_rng(77)
+    for trial in range(24):
+        n = int(rng.integers(1, 6000))
+        gv = rng.normal(size=(n, 3)) * rng.uniform(0.2, 2.0)
+        if trial % 4 == 1:                       # a lattice's g plus noise
+            a = rng.uniform(2.0, 9.0)
+            hkl = rng.integers(-6, 7, size=(n, 3)).astype(float)
+            q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            gv = (hkl / a) @ q.T + rng.normal(scale=1e-3, size=(n, 3))
+        m = int(rng.integers(1, 300))
+        ubis = np.empty((m, 3, 3))
+        for i in range(m):
+            q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            ubis[i] = np.diag(rng.uniform(1.5, 12.0, 3)) @ q.T
+        if trial % 4 == 2:                       # h exactly on half-integers for some g
+            gv[: n // 3] = np.linalg.solve(ubis[0], (rng.integers(-5, 5, (n // 3, 3)) + 0.5).T).T
+        tols = sorted(rng.uniform(0.001, 0.7, int(rng.integers(1, 5))).tolist())
+        c = B.score_grid(ubis, B.GvecGrid(gv), tols).cpu().numpy()
+        assert np.array_equal(c, oracle.score_many(ubis, gv, tols)), trial

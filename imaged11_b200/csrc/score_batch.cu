@@ -52,6 +52,11 @@ constexpr int kScoreR = ID11B_SCORE_UBIS_PER_THREAD;
 #define ID11B_SCORE_UNROLL 4
 #endif
 constexpr int kScoreUnroll = ID11B_SCORE_UNROLL;
+// counts-only screening with register counters where a CTA's g range allows
+// (20,000 UBIs x 1.1M g on B200: 16.4 ms against 16.9 ms with shared counters)
+#ifndef ID11B_SCORE_REGCOUNT
+#define ID11B_SCORE_REGCOUNT 1
+#endif
 // resident CTAs per SM the screening kernel is compiled for (register budget)
 __host__ __device__ constexpr int score_ctas_per_sm(int r) { return r <= 2 ? 4 : r <= 4 ? 3 : 2; }
 constexpr int kTile = 1024;         // g per TMA tile (16 KB of float4)
@@ -247,8 +252,10 @@ __device__ __forceinline__ uint64_t drlv2_pair(const uint64_t up[9], uint64_t gx
 
 // ------------------------------------------------------------ main kernel --
 // SUMS = false (MODE_SCORE without a sums output): the rare path counts only
-// and the float sums are not even allocated.
-template <int R, int NT, int MODE, bool SUMS = true>
+// and the float sums are not even allocated.  REGC (with SUMS = false, when a
+// CTA's g range is below 65,536): the counts live in registers, two 16-bit
+// counters per 32-bit register, instead of shared memory.
+template <int R, int NT, int MODE, bool SUMS = true, bool REGC = false>
 __global__ void __launch_bounds__(kBT, MODE == MODE_SCORE ? score_ctas_per_sm(R) : 2)
 k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ g4,
         const double* __restrict__ gv, const double* __restrict__ ubis, int64_t n, int gsplit,
@@ -293,14 +300,20 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
     // consecutive words: MODE_SCORE int counts [NT] + float sums [NT]
     int* s_cnt = reinterpret_cast<int*>(s_acc);
     float* s_sum = reinterpret_cast<float*>(s_cnt + NT * kBT * R);
-    if (MODE == MODE_SCORE) {
+    static_assert(!REGC || (MODE == MODE_SCORE && !SUMS), "register counts: counts only");
+    unsigned pc[R][(NT + 1) / 2];
+#pragma unroll
+    for (int r = 0; r < R; r++)
+#pragma unroll
+        for (int q = 0; q < (NT + 1) / 2; q++) pc[r][q] = 0u;
+    if (MODE == MODE_SCORE && !REGC) {
         for (int j = 0; j < NT; j++)
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 s_cnt[j * (kBT * R) + r * kBT + tid] = 0;
                 if (SUMS) s_sum[j * (kBT * R) + r * kBT + tid] = 0.f;  // absent otherwise
             }
-    } else {
+    } else if (MODE == MODE_REFINE) {  // (REGC allocates no shared accumulators at all)
         for (int f = 0; f < 17; f++)
 #pragma unroll
             for (int r = 0; r < R; r++) s_acc[f * (kBT * R) + r * kBT + tid] = 0.;
@@ -353,8 +366,12 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
                         for (int j = 0; j < NT; j++) {
                             const int slot = j * (kBT * R) + r * kBT + tid;
                             if (s[r] < band.lo[j]) {
-                                s_cnt[slot]++;
-                                if (SUMS) s_sum[slot] += s[r];
+                                if (REGC) {
+                                    pc[r][j >> 1] += 1u << ((j & 1) * 16);
+                                } else {
+                                    s_cnt[slot]++;
+                                    if (SUMS) s_sum[slot] += s[r];
+                                }
                             } else if (s[r] < band.hi[j]) {
                                 double uu[9], ihd[3];
 #pragma unroll
@@ -363,8 +380,12 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
                                                          gv[3 * gk + 2], ihd);
                                 atomicAdd(&ui->nrecheck, 1ull);
                                 if (s64 < tols.t[j] * tols.t[j]) {
-                                    s_cnt[slot]++;
-                                    if (SUMS) s_sum[slot] += (float)s64;
+                                    if (REGC) {
+                                        pc[r][j >> 1] += 1u << ((j & 1) * 16);
+                                    } else {
+                                        s_cnt[slot]++;
+                                        if (SUMS) s_sum[slot] += (float)s64;
+                                    }
                                 }
                             }
                         }
@@ -419,7 +440,17 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
         return;
     }
 
-    if (MODE == MODE_SCORE) {
+    if (REGC) {
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            if (mi[r] >= m) continue;
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                const int c = (int)((pc[r][j >> 1] >> ((j & 1) * 16)) & 0xffffu);
+                if (c) atomicAdd(counts + mi[r] * NT + j, c);
+            }
+        }
+    } else if (MODE == MODE_SCORE) {
 #pragma unroll
         for (int r = 0; r < R; r++) {
             if (mi[r] >= m) continue;
@@ -587,7 +618,7 @@ static UbiWs ubi_ws_layout(void* base, int64_t m, int64_t n, int mode) {
     return w;
 }
 
-template <int R, int NT, int MODE, bool SUMS = true>
+template <int R, int NT, int MODE, bool SUMS = true, bool REGC = false>
 static void launch_batch(int64_t m, int64_t n, int gsplit, const float4* packs, const float4* g4,
                          const double* gv, const double* ubis, const Tols& tols,
                          const GvecInfo* gi, UbiInfo* ui, int* counts, double* sums,
@@ -595,8 +626,9 @@ static void launch_batch(int64_t m, int64_t n, int gsplit, const float4* packs, 
     static_assert(MODE == MODE_SCORE || R == 2, "refinement keeps two UBIs per thread");
     const int64_t ublocks = (m + kBT * R - 1) / (kBT * R);
     size_t dyn = MODE == MODE_REFINE ? sizeof(double) * 17 * kBT * R
-                                     : (sizeof(int) + (SUMS ? sizeof(float) : 0)) * NT * kBT * R;
-    auto kern = k_batch<R, NT, MODE, SUMS>;
+                 : REGC ? 0
+                        : (sizeof(int) + (SUMS ? sizeof(float) : 0)) * NT * kBT * R;
+    auto kern = k_batch<R, NT, MODE, SUMS, REGC>;
     // static (32 KB of tiles) + dynamic exceeds the 48 KB default: opt in once
     static bool attr_set = false;
     if (!attr_set) {
@@ -698,6 +730,13 @@ static void launch_score(int ntol, int64_t m, int64_t n, int gsplit, const UbiWs
             case 2: launch_batch<R, 2, MODE_SCORE, true>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
             case 3: launch_batch<R, 3, MODE_SCORE, true>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
             default: launch_batch<R, 4, MODE_SCORE, true>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, sums, nullptr, st); break;
+        }
+    } else if (ID11B_SCORE_REGCOUNT && ((((n + gsplit - 1) / gsplit) + 3) & ~(int64_t)3) < 65536) {
+        switch (ntol) {  // a CTA counts below 65,536 g: 16-bit register counters suffice
+            case 1: launch_batch<R, 1, MODE_SCORE, false, true>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, nullptr, nullptr, st); break;
+            case 2: launch_batch<R, 2, MODE_SCORE, false, true>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, nullptr, nullptr, st); break;
+            case 3: launch_batch<R, 3, MODE_SCORE, false, true>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, nullptr, nullptr, st); break;
+            default: launch_batch<R, 4, MODE_SCORE, false, true>(m, n, gsplit, w.packs, g4, gv, ubis, T, gi, w.info, counts, nullptr, nullptr, st); break;
         }
     } else {
         switch (ntol) {

@@ -32,7 +32,7 @@ def build(verbose=False, extra=(), out=None, objdir=None):
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
         cmd = [NVCC, *ARCH, *FLAGS, *extra, "-I", os.path.join(HERE, "..", "include"),
-               "-dc" if False else "-c", src, "-o", obj]
+               "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -12,6 +12,8 @@
 // Also the plain batched FP64 scorer (many UBIs x many g, one launch per
 // tolerance set), the baseline against which the batched FP32 kernels are
 // measured.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "common.cuh"
@@ -387,12 +389,17 @@ extern "C" int id11b_dev_score_many_fp64(const double* ubis, int64_t m, const do
 // ------------------------------------------------ allocation-free variant ----
 // score_and_refine for callers that must not allocate device memory: a
 // process that reserves the GPU's memory up front for detector frame buffers
-// and forbids later allocations (to keep acquisition latency predictable), a
-// host that runs this code inside another framework's memory pool with a hard
-// cap, or code called back from a stream where no allocating CUDA call may be
-// made.  The least-squares partial sums live in this file-scope device array
-// (kLsqMaxBlocks x 136 bytes = 136 KiB, held by every GPU that loads the
+// and forbids later allocations (to keep acquisition latency predictable), or
+// a host that runs this code inside another framework's memory pool with a
+// hard cap.  The least-squares partial sums live in this file-scope device
+// array (kLsqMaxBlocks x 136 bytes = 136 KiB, held by every GPU that loads the
 // library until the process exits) instead of caller- or pool-provided memory.
+//
+// CUDA loads modules lazily (the default since CUDA 12.2): the module holding
+// this array and the kernels below is loaded, and its memory taken, on the
+// first call in each context.  A caller that reserves memory or caps a pool
+// afterwards makes one warm-up call per device first (one g-vector is enough;
+// it launches both kernels).
 //
 // Every call on a device shares the array.  Each partial-sum CTA writes its own
 // slot before the finishing CTA reads it, so the previous call's contents never
@@ -402,25 +409,71 @@ extern "C" int id11b_dev_score_many_fp64(const double* ubis, int64_t m, const do
 static __device__ __align__(256) LsqPartial g_lsq_scratch[kLsqMaxBlocks];
 
 namespace {
-constexpr int kMaxDevices = 64;
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// The array's device address belongs to the context the module was loaded
+// in: a driver-API caller's own context, or a primary context recreated after
+// cudaDeviceReset, holds it elsewhere.  So the cache is keyed by the unique id
+// of the current context (cuCtxGetId), never by the device ordinal.
+constexpr int kMaxContexts = 64;
+struct ScratchEntry {
+    unsigned long long ctx_id;
+    void* ptr;
+};
 std::mutex g_lsq_scratch_mu;
-void* g_lsq_scratch_ptr[kMaxDevices] = {};  // device address of g_lsq_scratch, per device
+ScratchEntry g_lsq_scratch_cache[kMaxContexts] = {};
+int g_lsq_scratch_used = 0;
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+int driver_entry_points() {  // under g_lsq_scratch_mu
+    if (g_ctx_get_current && g_ctx_get_id) return ID11B_OK;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return id11b_record_cuda(e);
+    if (q != cudaDriverEntryPointSuccess || !f) return ID11B_ERR_CUDA;
+    g_ctx_get_current = (CtxGetCurrentFn)f;
+    f = nullptr;
+    e = cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return id11b_record_cuda(e);
+    if (q != cudaDriverEntryPointSuccess || !f) return ID11B_ERR_CUDA;
+    g_ctx_get_id = (CtxGetIdFn)f;
+    return ID11B_OK;
+}
 
 // The name g_lsq_scratch is only a host-side stand-in: a kernel must be given
-// the device address, looked up once per device with that device current.
+// the device address, looked up with the context current in which it runs.
 int lsq_scratch_address(void** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return id11b_record_cuda(e);
-    if (dev < 0 || dev >= kMaxDevices) return ID11B_ERR_SIZE;
     std::lock_guard<std::mutex> lock(g_lsq_scratch_mu);
-    if (!g_lsq_scratch_ptr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_lsq_scratch);
-        if (e != cudaSuccess) return id11b_record_cuda(e);
-        g_lsq_scratch_ptr[dev] = p;
+    int rc = driver_entry_points();
+    if (rc) return rc;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    void* p = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS) return ID11B_ERR_CUDA;
+    if (ctx) {
+        if (g_ctx_get_id(ctx, &id) != CUDA_SUCCESS) return ID11B_ERR_CUDA;
+        for (int i = 0; i < g_lsq_scratch_used; i++)
+            if (g_lsq_scratch_cache[i].ctx_id == id) {
+                *out = g_lsq_scratch_cache[i].ptr;
+                return ID11B_OK;
+            }
     }
-    *out = g_lsq_scratch_ptr[dev];
+    // with no context current yet, this runtime call makes the current
+    // device's primary context current first
+    cudaError_t e = cudaGetSymbolAddress(&p, g_lsq_scratch);
+    if (e != cudaSuccess) return id11b_record_cuda(e);
+    if (!ctx) {
+        if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return ID11B_ERR_CUDA;
+        if (g_ctx_get_id(ctx, &id) != CUDA_SUCCESS) return ID11B_ERR_CUDA;
+    }
+    // context ids are never reused; past kMaxContexts the oldest slot is replaced
+    const int slot = g_lsq_scratch_used < kMaxContexts ? g_lsq_scratch_used++
+                                                       : (int)(id % kMaxContexts);
+    g_lsq_scratch_cache[slot] = ScratchEntry{id, p};
+    *out = p;
     return ID11B_OK;
 }
 }  // namespace

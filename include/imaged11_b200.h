@@ -145,16 +145,19 @@ int id11b_dev_refine_assigned(double *ubi, const double *gv, const int32_t *labe
 
 /* No counterpart in the reference.  score_and_refine on device pointers that
  * allocates nothing, for callers that cannot allocate device memory (a process
- * that has reserved the GPU's memory up front and forbids later allocations, a
- * host running inside another framework's capped memory pool, code called from
- * a stream where allocating CUDA calls are not allowed).  Same arguments and
- * results as id11b_dev_score_and_refine minus the workspace: the scratch is a
- * library-owned device array of id11b_noalloc_scratch_bytes() bytes (136 KiB)
- * that every GPU loading the library holds until the process exits.  The first
- * call on a device looks up that array's device address; make it before any
- * stream capture.  ng beyond 2^31-1 returns ID11B_ERR_SIZE.  All calls on a
- * device share the array: calls that overlap on the GPU race, so serialise
- * them (one stream, or explicit ordering). */
+ * that has reserved the GPU's memory up front and forbids later allocations, or
+ * a host running inside another framework's capped memory pool).  Same
+ * arguments and results as id11b_dev_score_and_refine minus the workspace: the
+ * scratch is a library-owned device array of id11b_noalloc_scratch_bytes()
+ * bytes (136 KiB) that every GPU loading the library holds until the process
+ * exits.  CUDA loads the module holding that array lazily, so the first call in
+ * each context takes device memory: make one warm-up call per device (one
+ * g-vector is enough) before reserving memory or capping the pool, and before
+ * any stream capture.  The array's device address is cached per CUDA context
+ * (a context recreated after cudaDeviceReset is looked up afresh).  ng beyond
+ * 2^31-1 returns ID11B_ERR_SIZE.  All calls on a device share the array: calls
+ * that overlap on the GPU race, so serialise them (one stream, or explicit
+ * ordering). */
 int64_t id11b_noalloc_scratch_bytes(void);
 int id11b_dev_score_and_refine_noalloc(double *ubi, const double *gv, double tol, int64_t ng,
                                        int32_t *n, double *mean_drlv2, void *stream);

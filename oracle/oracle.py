@@ -219,10 +219,13 @@ class Reference(_Lib):
         return int(self.lib.ref_max_threads())
 
 
-def build(ref_root="/root/reference"):
-    """Compile liboracle.so, and the reference library when its sources exist."""
+def build(ref_root=None):
+    """Compile liboracle.so, and the reference library when its sources exist
+    (ref_root, else the IMAGED11_REF environment variable: the root of an
+    ImageD11 checkout; with neither, only the restatement is built)."""
     import subprocess
     cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+    ref_root = ref_root or os.environ.get("IMAGED11_REF", "")
     subprocess.run(["make", "-s", "-C", HERE, "CC=" + cc, "REF=" + ref_root],
                    check=True)
 

@@ -1,10 +1,11 @@
 """Generate the golden fixtures in tests/golden/ from the REFERENCE itself.
 
-Run in a container that has the reference checkout (default /root/reference):
+Run where an ImageD11 checkout exists, naming its root (argument or the
+IMAGED11_REF environment variable):
 
-    make -C oracle            # builds oracle/_ref/libimaged11_ref.so from the
-                              # reference's own src/closest.c, src/cdiffraction.c
-    python tests/golden/make_golden.py [/path/to/reference]
+    make -C oracle REF=/path/to/ImageD11   # builds oracle/_ref/libimaged11_ref.so
+                                           # from the reference's own C sources
+    python tests/golden/make_golden.py /path/to/ImageD11
 
 Outputs come from two reference implementations:
 
@@ -292,7 +293,9 @@ def cases_adjoint(tr):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("IMAGED11_REF")
+    if not ref_root:
+        sys.exit("usage: make_golden.py /path/to/ImageD11 (or set IMAGED11_REF)")
     ref = Reference()
     tr = import_reference_transform(ref_root)
     assert ref.verify_rounding(20) == 0

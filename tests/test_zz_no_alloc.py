@@ -77,3 +77,27 @@ def test_noalloc_rejects_sizes_beyond_maximum(cuda):
     rc = lib.id11b_dev_score_and_refine_noalloc(8, 8, 0.1, 2 ** 31, 8, 8, None)
     assert rc == 4   # ID11B_ERR_SIZE
     assert lib.id11b_dev_score_and_refine_noalloc(8, 8, 0.1, -1, 8, 8, None) == 1
+
+
+def test_noalloc_warmed_call_takes_no_device_memory(golden, cuda):
+    """After one warm-up call (which loads the library's module lazily), a call
+    leaves the device's free memory unchanged: the entry point allocates nothing."""
+    import torch
+    from imaged11_b200._lib import lib
+    d = golden["scoring"]
+    gv = torch.tensor(d["sc_gv"], device=cuda)
+    ub = torch.tensor(d["sc_ubis"][5], dtype=torch.float64, device=cuda).contiguous()
+    n = torch.zeros(1, dtype=torch.int32, device=cuda)
+    m = torch.zeros(1, dtype=torch.float64, device=cuda)
+    stream = torch.cuda.current_stream().cuda_stream
+    fn = lib.id11b_dev_score_and_refine_noalloc
+    assert fn(ub.data_ptr(), gv.data_ptr(), 0.05, gv.shape[0], n.data_ptr(), m.data_ptr(),
+              stream) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(cuda)
+    for _ in range(3):
+        assert fn(ub.data_ptr(), gv.data_ptr(), 0.05, gv.shape[0], n.data_ptr(),
+                  m.data_ptr(), stream) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(cuda)
+    assert free1 == free0

@@ -63,6 +63,9 @@ _SIGNATURES = [
     ("id11b_dev_score_grid", _i, [_p, _i64, _p, _i64, _i, _i, _p, _p, _i, _p, _p, _p, _i64,
                                    _p]),
     ("id11b_grid_stats", _i, [_p, _p, _p, _p, _p, _p]),
+    ("id11b_grid_bins_workspace_bytes", _i64, [_i64, _i, _i, _i64]),
+    ("id11b_dev_score_grid_bins", _i, [_p, _i64, _p, _i64, _i, _i, _p, _p, _i, _p, _p, _p,
+                                        _i64, _p]),
     ("id11b_grid_refine_workspace_bytes", _i64, [_i64]),
     ("id11b_dev_refine_grid", _i, [_p, _i64, _p, _i64, _i, _i, _p, _d, _i, _p, _p, _p, _i64,
                                     _p]),

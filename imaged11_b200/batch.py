@@ -22,6 +22,8 @@ import numpy as np
 
 from ._lib import lib, check
 
+ID11B_ERR_SIZE = 4
+
 
 def _torch():
     import torch
@@ -184,20 +186,101 @@ class GvecGrid:
                         (x.value for x in v)))
 
 
-def score_grid(ubis, grid, tols, sums=False, workspace=None, out=None):
+BINS_TOL_LIMIT = 0.4   # the binned join takes tolerances below this
+BINS_MAX_BOXES = 1 << 29   # default workspace cap (4 GiB of boxes); more run in UBI ranges
+BINS_MAX_ROWS = 16384      # the binned join holds nx^2 rows of cells ...
+BINS_MAX_XCELLS = 8191     # ... and nx * xsub x cells per row
+
+
+def bins_fit(grid):
+    """Whether the binned join takes this grid's shape."""
+    return grid.nx * grid.nx <= BINS_MAX_ROWS and grid.nx * grid.xsub <= BINS_MAX_XCELLS
+
+
+def bins_box_estimate(ubis, grid, tmax):
+    """An estimate (about 25 % above the expected count) of the (UBI, hkl)
+    boxes the binned join enumerates for these UBIs: the lattice points of
+    each UBI within rmax + |w| of the origin.  Reads one number back."""
+    torch = _torch()
+    u = _dev(ubis, torch.float64).reshape(-1, 3, 3)
+    if u.shape[0] == 0:
+        return 0
+    det = torch.nan_to_num(torch.linalg.det(u).abs(), nan=0.0, posinf=0.0)
+    ok = det > 0
+    ub = torch.linalg.inv(torch.where(ok[:, None, None], u, torch.eye(3, dtype=u.dtype,
+                                                                    device=u.device)))
+    w = (tmax + 1e-6) * ub.norm(dim=2).norm(dim=1)
+    r = grid.rmax + torch.nan_to_num(w, nan=0.0, posinf=0.0)
+    est = (4.0 / 3.0 * np.pi) * (r ** 3) * det * ok
+    # a UBI with more candidate hkl than g-vectors, or a large row sum, is
+    # scanned plainly and enumerates no boxes
+    est = torch.where(est <= grid.n, est, torch.zeros_like(est))
+    total = 1.25 * float(est.sum().item()) + 64 * u.shape[0]
+    return int(min(total, BINS_MAX_BOXES))
+
+
+class BinsWorkspace:
+    """Reusable scratch of the binned join for m UBIs on a grid, holding
+    `boxes` (UBI, hkl) boxes at a time (a shorter workspace still works: the
+    UBIs are then processed in ranges that fit)."""
+
+    def __init__(self, m, grid, boxes):
+        torch = _torch()
+        self.m, self.nx, self.xsub, self.boxes = m, grid.nx, grid.xsub, int(boxes)
+        nbytes = lib.id11b_grid_bins_workspace_bytes(m, grid.nx, grid.xsub, self.boxes)
+        if nbytes < 0:
+            raise ValueError("bad binned-join workspace size")
+        self.buf = torch.empty(nbytes, dtype=torch.uint8, device=grid.gv.device)
+
+    def fits(self, m, grid, boxes):
+        return lib.id11b_grid_bins_workspace_bytes(m, grid.nx, grid.xsub, int(boxes)) <= \
+            self.buf.numel()
+
+
+def score_grid(ubis, grid, tols, sums=False, workspace=None, out=None, method=None):
     """score_batch through the cell index: the same counts (and, with
     sums=True, FP64 sums of the counted drlv2) for every UBI and tolerance,
-    testing only the g-vectors near each UB.hkl.  grid: GvecGrid."""
+    testing only the g-vectors near each UB.hkl.  grid: GvecGrid.
+
+    method "bins" (the default when every tolerance is below 0.4): the binned
+    join, every (UBI, hkl) box against the g of its bin's region in FP32 with
+    the proven FP64 recheck band (its sums' last bits depend on the order of
+    the atomics); "walk": per-box lookups with every candidate evaluated in
+    FP64 (any tolerance, sums in a fixed order).  workspace: a BinsWorkspace
+    ("bins") or a uint8 CUDA tensor ("walk")."""
     torch = _torch()
     u = _dev(ubis, torch.float64).reshape(-1, 9)
     m = u.shape[0]
     t = _tols(tols)
-    need = lib.id11b_grid_score_workspace_bytes(m, len(t))
-    ws = workspace if workspace is not None and workspace.numel() >= need else \
-        torch.empty(need, dtype=torch.uint8, device=u.device)
+    auto = method is None
+    if auto:
+        method = "bins" if float(t.max()) < BINS_TOL_LIMIT and bins_fit(grid) else "walk"
+    elif method == "bins" and not bins_fit(grid):
+        raise ValueError("the binned join holds at most %d rows of %d x cells; use "
+                         "method='walk' or coarser cells" % (BINS_MAX_ROWS, BINS_MAX_XCELLS))
     counts = out if out is not None else torch.empty((m, len(t)), dtype=torch.int32,
                                                      device=u.device)
     s = torch.empty((m, len(t)), dtype=torch.float64, device=u.device) if sums else None
+    if method == "bins":
+        ws = workspace if isinstance(workspace, BinsWorkspace) and workspace.m >= m and \
+            (workspace.nx, workspace.xsub) == (grid.nx, grid.xsub) else None
+        if ws is None:
+            ws = BinsWorkspace(m, grid, bins_box_estimate(u, grid, float(t.max())))
+        rc = lib.id11b_dev_score_grid_bins(u.data_ptr(), m, grid.gv.data_ptr(), grid.n,
+                                           grid.nx, grid.xsub, grid.buf.data_ptr(),
+                                           t.ctypes.data, len(t), counts.data_ptr(),
+                                           s.data_ptr() if sums else None, ws.buf.data_ptr(),
+                                           ws.buf.numel(), _stream())
+        score_grid.last_workspace = ws
+        if not (auto and rc == ID11B_ERR_SIZE):   # cells far smaller than the boxes: walk
+            check(rc, "score_grid_bins")
+            return (counts, s) if sums else counts
+        method = "walk"
+    if method != "walk":
+        raise ValueError("method: 'bins' or 'walk'")
+    need = lib.id11b_grid_score_workspace_bytes(m, len(t))
+    ws = workspace if workspace is not None and not isinstance(workspace, BinsWorkspace) and \
+        workspace.numel() >= need else torch.empty(need, dtype=torch.uint8, device=u.device)
     check(lib.id11b_dev_score_grid(u.data_ptr(), m, grid.gv.data_ptr(), grid.n, grid.nx,
                                    grid.xsub, grid.buf.data_ptr(), t.ctypes.data, len(t), counts.data_ptr(),
                                    s.data_ptr() if sums else None, ws.data_ptr(), ws.numel(),

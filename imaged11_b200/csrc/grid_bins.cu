@@ -1,0 +1,969 @@
+// Binned scoring through the reciprocal-space cell index: a spatial join of
+// (UBI, hkl) boxes with the g-vectors.
+//
+// score() (ImageD11 src/closest.c:227-248) counts, for one UBI, the g with
+// |UBI.g - round(UBI.g)|^2 < tol^2.  Such a g lies in the box
+// [UB.hkl - w, UB.hkl + w] of its own hkl = round(UBI.g) (grid.cuh: the half
+// widths w are conservative).  Here every box that can reach the data is
+// enumerated once per UBI (the lookup scorer's enumeration, its per-candidate
+// work in FP32 with the rounding folded into w) and the boxes are sorted by
+// the row of grid cells holding their centre (fixed y and z cell): counts per
+// row in shared memory per CTA, a scan, and a second enumeration that writes
+// each CTA's boxes of a row as one contiguous run.  One CTA then takes one
+// row: it sorts the row's boxes by x cell in shared memory, stages the
+// g-vectors of the row's region (its y/z cell widened by the largest half
+// width W, all x cells the boxes need) sorted by x cell, and every run of 32
+// boxes (a warp, one box per lane) is tested against the contiguous range of
+// staged g whose x cells its boxes can reach.  Each lane holds its box's UBI
+// in FP32 registers, duplicated into packed pairs, and its hkl; two staged g
+// are read by all lanes at once (broadcast) and tested with packed f32x2
+// instructions.
+//
+// Per (box, g), the screening kernel's FP32 arithmetic (score_batch.cu):
+//   h = UBI32 . g32 (FMA chains),  d = h - hkl,  s = d.d;
+//   s < lo_j           -> counted for tolerance j,
+//   lo_j <= s < hi_j   -> re-evaluated with the reference's exact FP64
+//                         arithmetic, counted when drlv2 < tol_j^2 and the
+//                         rounded h is the box's hkl,
+//   s >= hi_j          -> not counted for j.
+// The band [lo_j, hi_j) is the screening kernel's proven one, from
+// |h32 - h64| <= E = 6 * 2^-24 * S * gmax (S = largest row sum of |UBI|).
+// With every tolerance below 0.4 and S * gmax < 16384 (E < 0.006), a pair
+// with s < hi_j has all |d| < 0.45, so h - hkl is exact in FP32 (Sterbenz),
+// the FP32 value is the screening kernel's, and for s < lo_j the rounded h64
+// is hkl and drlv2 < tol_j^2: the pair is counted under its own hkl exactly
+// when the reference counts it.  A pair tested against a box of another hkl
+// has some |d| >= 0.5 - E, so s >= 0.2 > hi_j: never counted.  A staged tile
+// holds each g once, so no pair is tested twice in a tile, and every g of a
+// row's region lies in exactly one tile.
+//
+// UBIs outside the limits (the lookup plan's caps, hkl beyond -256..255,
+// S * gmax too large) are scored by an exact FP64 scan of every regular g, and
+// the g-vectors outside the regular range by an exact FP64 scan of their list.
+// Counts go to the output with integer atomics (exact); the optional FP64
+// sums of the counted drlv2 are added with double atomics, so their last bits
+// depend on the order the warps finish in.
+#include <math.h>
+#include <string.h>
+#include <algorithm>
+#include <vector>
+
+#include "grid.cuh"
+
+namespace id11b {
+namespace grid {
+namespace bins {
+
+constexpr int kEW = 8;              // warps per enumeration CTA
+constexpr int kET = 32 * kEW;
+constexpr int kJT = 256;            // threads per join CTA (one row at a time)
+constexpr int kJW = kJT / 32;
+constexpr int kBMax = 4096;         // boxes of a row sorted in shared memory at a time
+constexpr int kGMax = 2048;         // g staged at a time (one tile)
+constexpr int kMaxRows = 16384;     // rows of cells (nx^2) the enumeration's counters hold
+constexpr int kMaxNxx = 8191;       // x cells per row (13-bit field of a box record)
+constexpr int kMaxHalo = 1024;      // rows of cells around a row (the halo R: (2R+1)^2)
+constexpr int kMaxEnumCtas = 512;
+constexpr double kTolLimit = 0.4;
+constexpr double kSGLimit = 16384.0;
+constexpr double kEps32 = 5.9604644775390625e-08;  // 2^-24
+constexpr int kHklOff = 256;        // hkl in 9-bit fields: -256 .. 255
+constexpr int kUbiBits = 24;        // UBI index (within a range of UBIs) in a box record
+constexpr int kFallbackParts = 128; // warps per plainly scanned UBI
+constexpr int kBT = 128;            // threads per CTA of the exact scans
+constexpr int kBW = kBT / 32;
+#ifndef ID11B_JOIN_MINB
+#define ID11B_JOIN_MINB 3
+#endif
+constexpr int kJoinMinBlocks = ID11B_JOIN_MINB;  // resident join CTAs per SM compiled for
+
+struct BinInfo {
+    unsigned long long wmax_bits;  // largest (widened) box half width (positive doubles order as integers)
+    unsigned long long total;      // boxes enumerated by the first counting pass
+    unsigned int smax_bits;        // largest row sum of |UBI| over binned UBIs (float, rounded up)
+    int nfallback;                 // UBIs scored by the plain scan
+    int next_row;                  // row counter of the join
+    int pad;
+};
+
+// Everything the join needs that is uniform over the launch, computed on the
+// host after the counting pass (kernel parameters: no registers).
+struct JoinParams {
+    float lo[ID11B_MAX_TOLS], hi[ID11B_MAX_TOLS];
+    double t2[ID11B_MAX_TOLS];
+    float hmax;
+    // y/z region of row (iy, iz): [rlo + iy * cs, rhi + (iy + 1) * cs] (the
+    // cell widened by W + eps; eps covers the FP32 rounding of the box
+    // centres' cells and of these bounds); the halo in whole cells
+    float rlo, rhi, cs;
+    int R, Rx, nx, nxx;
+    int64_t i0;                    // first UBI of the range (box records are relative to it)
+};
+
+// box record: UBI (24 bits, relative) | h + 256 (9) | k + 256 (9) | l + 256 (9) | x cell (13)
+__device__ __forceinline__ uint64_t pack_box(int64_t u, int h, int k, int l, int fx) {
+    return ((uint64_t)u << 40) | ((uint64_t)(h + kHklOff) << 31) |
+           ((uint64_t)(k + kHklOff) << 22) | ((uint64_t)(l + kHklOff) << 13) | (uint64_t)fx;
+}
+__device__ __forceinline__ int box_fx(uint64_t r) { return (int)(r & 8191u); }
+
+struct BinLayout {
+    size_t info, packs, cnt_ubi, fallback, cta_rows, rowtot, rstart, tot, recs, bytes;
+};
+
+// workspace: info | packs (m x 3 float4) | per-UBI box counts | fallback list |
+// per-CTA row counts / offsets | row totals | row starts | scan totals | boxes
+inline BinLayout bin_layout(int64_t m, int64_t nrows, int64_t cap) {
+    BinLayout L;
+    const size_t mm = (size_t)(m > 0 ? m : 1);
+    size_t o = 0;
+    L.info = o;     o = al256(o + sizeof(BinInfo));
+    L.packs = o;    o = al256(o + 3 * sizeof(float4) * mm);
+    L.cnt_ubi = o;  o = al256(o + sizeof(int) * mm);
+    L.fallback = o; o = al256(o + sizeof(int) * mm);
+    L.cta_rows = o; o = al256(o + sizeof(int) * (size_t)kMaxEnumCtas * (size_t)nrows);
+    L.rowtot = o;   o = al256(o + sizeof(int) * (size_t)(nrows + 1));
+    L.rstart = o;   o = al256(o + sizeof(int) * (size_t)(nrows + 1));
+    L.tot = o;      o = al256(o + sizeof(int) * (size_t)((nrows + 1 + kScanPer - 1) / kScanPer + 1));
+    L.recs = o;     o = al256(o + sizeof(uint64_t) * (size_t)(cap > 0 ? cap : 1));
+    L.bytes = o;
+    return L;
+}
+
+// packed FP32 pairs (sm_100 f32x2): every lane does exactly the scalar operation
+__device__ __forceinline__ uint64_t pk2(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk2(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// FP32 form of a UBI's plan for the candidate work of the enumeration.  The
+// half widths are widened by a bound on the FP32 error of the box centre:
+// c = fma(l, ub_r2, fma(k, ub_r1, h * ub_r0)) with ub rounded to FP32 is
+// within 4 * 2^-24 * max|hkl| * sum_j |ub_rj| of UB.hkl (input rounding plus
+// three roundings of partial sums no larger than that sum), so every box
+// [c - w', c + w'] holds the exact one, and every test on it is conservative.
+struct Plan32 {
+    float ub[9], w[3];
+    float G, rmax2;       // cube half side and squared radius, rounded up
+};
+
+__device__ __forceinline__ void make_plan32(const volatile WarpPlan* wp, const Header& H,
+                                            volatile Plan32* p, double* wmax) {
+    double hm = 0.;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+        hm = fmax(hm, fmax(fabs((double)wp->lo[r]), fabs((double)(wp->lo[r] + wp->nh[r] - 1))));
+    double wm = 0.;
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const double us = fabs(wp->ub[3 * r]) + fabs(wp->ub[3 * r + 1]) + fabs(wp->ub[3 * r + 2]);
+        const double err = 4.0 * kEps32 * hm * us * (1. + 1e-6);
+        const float wr = __double2float_ru(wp->w[r] + err);
+        p->w[r] = wr;
+        wm = fmax(wm, (double)wr);
+#pragma unroll
+        for (int j = 0; j < 3; j++) p->ub[3 * r + j] = __double2float_rn(wp->ub[3 * r + j]);
+    }
+    p->G = __double2float_ru(-H.lo * (1. + 1e-6));
+    p->rmax2 = __double2float_ru(H.rmax * H.rmax * (1. + 1e-5));
+    *wmax = wm;
+}
+
+// mode 0 counts the boxes per row of cells (and, in the first pass, writes
+// the plans' FP32 packs, the largest widened half width and row sum, the
+// per-UBI box counts and the fallback list); mode 1 writes every box.  CTA c
+// takes UBIs i0 + [c * per, (c + 1) * per), its warps one UBI at a time in a
+// fixed order, and keeps one counter per row in shared memory: mode 0 stores
+// them in cta_rows[c][row]; mode 1 starts them at rstart[row] + cta_rows[c][row]
+// (the CTA's offset inside the row) and writes each box at its counter.  The
+// mode is a run-time argument of one kernel, so both passes run the same
+// machine code and put every box in the same row; each write is still bounded
+// by its row's range.
+__global__ void __launch_bounds__(kET)
+k_enum(int mode, const double* __restrict__ ubis, int64_t i0, int64_t mc, int64_t per,
+       const Header* __restrict__ Hp, const int* __restrict__ start, double tmax, int first,
+       int nrows, BinInfo* __restrict__ info, float4* __restrict__ packs,
+       int* __restrict__ cnt_ubi, int* __restrict__ fallback, int* __restrict__ cta_rows,
+       const int* __restrict__ rstart, uint64_t* __restrict__ recs) {
+    extern __shared__ int s_rows[];
+    __shared__ WarpPlan s_plan[kEW];
+    __shared__ Plan32 s_p32[kEW];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int* my = cta_rows + (int64_t)blockIdx.x * nrows;
+    for (int r = threadIdx.x; r < nrows; r += kET) s_rows[r] = mode == 0 ? 0 : rstart[r] + my[r];
+    __syncthreads();
+    const Header H = *Hp;
+    const int64_t nreg = start[H.ncells];
+    const float flo = (float)H.lo, inv_cs = (float)H.inv_cs, inv_csx = (float)H.inv_csx;
+    const int64_t u1 = min((int64_t)(blockIdx.x + 1) * per, mc);
+    volatile WarpPlan* wp = s_plan + w;
+    volatile Plan32* p32 = s_p32 + w;
+    for (int64_t u = (int64_t)blockIdx.x * per + w; u < u1; u += kEW) {
+        const int64_t i = i0 + u;
+        bool ok = setup_plan(wp, ubis, i, tmax, H, nreg, lane);
+        double smax = 0.;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            smax = fmax(smax, fabs(wp->u[3 * r]) + fabs(wp->u[3 * r + 1]) + fabs(wp->u[3 * r + 2]));
+            ok = ok && wp->lo[r] >= -kHklOff && wp->lo[r] + wp->nh[r] - 1 < kHklOff;
+        }
+        smax *= 1. + 1e-15;
+        ok = ok && smax * (-H.lo) < kSGLimit;
+        const bool lead = mode == 0 && first && lane == 0;
+        if (!ok) {
+            if (lead) {
+                const int slot = atomicAdd(&info->nfallback, 1);
+                fallback[slot] = (int)i;
+            }
+            __syncwarp();
+            continue;
+        }
+        if (lane == 0) {
+            double wm;
+            make_plan32(wp, H, p32, &wm);
+            if (lead) {
+                float4* p = packs + 3 * i;
+                p[0] = make_float4(__double2float_rn(wp->u[0]), __double2float_rn(wp->u[1]),
+                                   __double2float_rn(wp->u[2]), __double2float_rn(wp->u[3]));
+                p[1] = make_float4(__double2float_rn(wp->u[4]), __double2float_rn(wp->u[5]),
+                                   __double2float_rn(wp->u[6]), __double2float_rn(wp->u[7]));
+                p[2] = make_float4(__double2float_rn(wp->u[8]), 0.f, 0.f, 0.f);
+                atomicMax(&info->smax_bits, __float_as_uint(__double2float_ru(smax)));
+                atomicMax(&info->wmax_bits, (unsigned long long)__double_as_longlong(wm));
+            }
+        }
+        __syncwarp();
+        // the FP32 plan in registers for the candidate loop
+        float ub[9], wr[3];
+#pragma unroll
+        for (int e = 0; e < 9; e++) ub[e] = p32->ub[e];
+#pragma unroll
+        for (int r = 0; r < 3; r++) wr[r] = p32->w[r];
+        const float G = p32->G, rmax2 = p32->rmax2;
+        int nbox = 0;
+        // the lookup enumeration's columns (FP64, flattened across the warp)
+        const int nh0 = wp->nh[0];
+        const int64_t nhk = (int64_t)nh0 * wp->nh[1];
+        const double R = (H.rmax + sqrt((double)wr[0] * wr[0] + (double)wr[1] * wr[1] +
+                                        (double)wr[2] * wr[2])) * (1. + 1e-9) + 1e-12;
+        for (int64_t hb = 0; hb < nhk; hb += 32) {
+            const int64_t hk = hb + lane;
+            int len = 0, l0 = 0, h = 0, k = 0;
+            if (hk < nhk) {
+                h = wp->lo[0] + (int)(hk % nh0);
+                k = wp->lo[1] + (int)(hk / nh0);
+                const double bx = wp->ub[2], by = wp->ub[5], bz = wp->ub[8];  // l direction
+                const double bb = bx * bx + by * by + bz * bz;
+                const double ax = wp->ub[0] * h + wp->ub[1] * k, ay = wp->ub[3] * h + wp->ub[4] * k,
+                             az = wp->ub[6] * h + wp->ub[7] * k;
+                const double ab = ax * bx + ay * by + az * bz;
+                const double aa = ax * ax + ay * ay + az * az;
+                const double disc = ab * ab - bb * (aa - R * R);
+                if (disc >= 0.) {
+                    // widened by one l on each side, far more than the rounding
+                    const double sq = sqrt(disc), ib = 1.0 / bb;
+                    const double la = fmax(floor((-ab - sq) * ib) - 1., (double)wp->lo[2]);
+                    const double lb = fmin(ceil((-ab + sq) * ib) + 1.,
+                                           (double)(wp->lo[2] + wp->nh[2] - 1));
+                    if (la <= lb) {
+                        l0 = (int)la;
+                        len = (int)(lb - la) + 1;
+                    }
+                }
+            }
+            int total;
+            const int excl = warp_excl_scan(len, lane, total);
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                const int f = f0 + lane;
+                const int j = owner(excl, f);
+                const int hj = __shfl_sync(0xffffffffu, h, j);
+                const int kj = __shfl_sync(0xffffffffu, k, j);
+                const int lj = __shfl_sync(0xffffffffu, l0, j) + f - __shfl_sync(0xffffffffu, excl, j);
+                if (f < total) {
+                    const float fh = (float)hj, fk = (float)kj, fl = (float)lj;
+                    float c[3], d2 = 0.f;
+                    bool in = true;
+#pragma unroll
+                    for (int r = 0; r < 3; r++) {
+                        c[r] = fmaf(fl, ub[3 * r + 2], fmaf(fk, ub[3 * r + 1], fh * ub[3 * r]));
+                        in = in && (c[r] - wr[r] <= G) && (c[r] + wr[r] >= -G);
+                        const float e = fmaxf(fabsf(c[r]) - wr[r], 0.f);
+                        d2 = fmaf(e, e, d2);
+                    }
+                    if (in && d2 <= rmax2) {
+                        const int cx = min(max(__float2int_rd((c[0] - flo) * inv_csx), 0), H.nxx - 1);
+                        const int cy = min(max(__float2int_rd((c[1] - flo) * inv_cs), 0), H.nx - 1);
+                        const int cz = min(max(__float2int_rd((c[2] - flo) * inv_cs), 0), H.nx - 1);
+                        const int row = cz * H.nx + cy;
+                        const int slot = atomicAdd(s_rows + row, 1);
+                        if (mode == 0) {
+                            nbox++;
+                        } else if (slot < rstart[row + 1]) {
+                            recs[slot] = pack_box(u, hj, kj, lj, cx);
+                        }
+                    }
+                }
+            }
+        }
+        if (mode == 0 && first) {
+            const int nb = warp_sum(nbox);
+            if (lane == 0) {
+                cnt_ubi[i] = nb;
+                if (nb) atomicAdd(&info->total, (unsigned long long)nb);
+            }
+        }
+    }
+    __syncthreads();
+    if (mode == 0)
+        for (int r = threadIdx.x; r < nrows; r += kET) my[r] = s_rows[r];
+}
+
+// Per row: the CTAs' counts turned into exclusive offsets inside the row (in
+// place), and the row's total.  One warp per row.
+__global__ void __launch_bounds__(kGT)
+k_row_offsets(int* __restrict__ cta_rows, int nctas, int nrows, int* __restrict__ rowtot) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t r = ((int64_t)blockIdx.x * kGT + threadIdx.x) >> 5; r < nrows;
+         r += ((int64_t)gridDim.x * kGT) >> 5) {
+        int run = 0;
+        for (int c0 = 0; c0 < nctas; c0 += 32) {
+            const int c = c0 + lane;
+            const int v = c < nctas ? cta_rows[(int64_t)c * nrows + r] : 0;
+            int tot;
+            const int ex = warp_excl_scan(v, lane, tot);
+            if (c < nctas) cta_rows[(int64_t)c * nrows + r] = run + ex;
+            run += tot;
+        }
+        if (lane == 0) rowtot[r] = run;
+    }
+}
+
+// ----------------------------------------------------------------- join ----
+// A pair inside a band (or, with sums, any pair below hmax): the reference's
+// exact FP64 drlv2.  Returns the tolerances (bit j) for which it counts and
+// its drlv2.  Out of line: rare, and its registers would otherwise weigh on
+// the whole join.
+template <int NT>
+__device__ __noinline__ unsigned exact_pair(const double* __restrict__ ubis, int64_t ubi,
+                                            const double* __restrict__ gs, int pos, float hk0,
+                                            float hk1, float hk2, const double* t2,
+                                            double* s64) {
+    double u[9], ih[3];
+#pragma unroll
+    for (int e = 0; e < 9; e++) u[e] = __ldg(ubis + 9 * ubi + e);
+    const double s = drlv2_exact(u, __ldg(gs + 3 * (int64_t)pos), __ldg(gs + 3 * (int64_t)pos + 1),
+                                 __ldg(gs + 3 * (int64_t)pos + 2), ih);
+    *s64 = s;
+    if (!(ih[0] == (double)hk0 && ih[1] == (double)hk1 && ih[2] == (double)hk2)) return 0u;
+    unsigned m = 0u;
+#pragma unroll
+    for (int j = 0; j < NT; j++)
+        if (s < t2[j]) m |= 1u << j;
+    return m;
+}
+
+// One screening value against the tolerances; rare pairs go exact.
+template <int NT, bool SUMS>
+__device__ __forceinline__ void count_pair(float s, const int* pos, const JoinParams& P,
+                                           const double* __restrict__ ubis, int64_t ubi,
+                                           const double* __restrict__ gs, const float* hkf,
+                                           int cnt[NT], double sum[NT], unsigned& ntest) {
+    bool exact = false;
+    if (SUMS) {
+        exact = s < P.hmax;
+    } else {
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+            const bool in = s < P.lo[j];
+            cnt[j] += in;
+            exact |= !in && s < P.hi[j];
+        }
+    }
+    if (exact) {
+        ntest++;
+        double s64;
+        const unsigned mk = exact_pair<NT>(ubis, ubi, gs, *pos, hkf[0], hkf[1], hkf[2], P.t2, &s64);
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+            if (SUMS) {
+                if (mk >> j & 1u) {
+                    cnt[j]++;
+                    sum[j] += s64;
+                }
+            } else if (!(s < P.lo[j]) && (mk >> j & 1u)) {
+                cnt[j]++;
+            }
+        }
+    }
+}
+
+struct Staged {  // the tile of staged g, structure of arrays (pairs read as 64 bits)
+    const float *x, *y, *z;
+    const int* pos;
+};
+
+// The box of one lane against staged g [ga, gb): a single g first if ga is
+// odd, then pairs with packed f32x2 instructions (the same operations as
+// drlv2_f32 lane by lane, so every screening value is the scalar one), then a
+// single last g.
+template <int NT, bool SUMS>
+__device__ __forceinline__ void test_range(const Staged& t, int ga, int gb, const float u[9],
+                                           const uint64_t uu[9], const uint64_t hh[3],
+                                           const float* hkf, const JoinParams& P,
+                                           const double* __restrict__ ubis, int64_t ubi,
+                                           const double* __restrict__ gs, int cnt[NT],
+                                           double sum[NT], unsigned& ntest) {
+    auto single = [&](int q) {
+        const float gx = t.x[q], gy = t.y[q], gz = t.z[q];
+        const float d0 = fmaf(u[2], gz, fmaf(u[1], gy, u[0] * gx)) - hkf[0];
+        const float d1 = fmaf(u[5], gz, fmaf(u[4], gy, u[3] * gx)) - hkf[1];
+        const float d2 = fmaf(u[8], gz, fmaf(u[7], gy, u[6] * gx)) - hkf[2];
+        count_pair<NT, SUMS>(fmaf(d2, d2, fmaf(d1, d1, d0 * d0)), t.pos + q, P, ubis, ubi, gs,
+                             hkf, cnt, sum, ntest);
+    };
+    int q = ga;
+    if (q < gb && (q & 1)) single(q++);
+    for (; q + 1 < gb; q += 2) {
+        const uint64_t gx = *reinterpret_cast<const uint64_t*>(t.x + q);
+        const uint64_t gy = *reinterpret_cast<const uint64_t*>(t.y + q);
+        const uint64_t gz = *reinterpret_cast<const uint64_t*>(t.z + q);
+        const uint64_t h0 = fma2(uu[2], gz, fma2(uu[1], gy, mul2(uu[0], gx)));
+        const uint64_t h1 = fma2(uu[5], gz, fma2(uu[4], gy, mul2(uu[3], gx)));
+        const uint64_t h2 = fma2(uu[8], gz, fma2(uu[7], gy, mul2(uu[6], gx)));
+        const uint64_t d0 = sub2(h0, hh[0]), d1 = sub2(h1, hh[1]), d2 = sub2(h2, hh[2]);
+        float sa, sb;
+        upk2(fma2(d2, d2, fma2(d1, d1, mul2(d0, d0))), sa, sb);
+        count_pair<NT, SUMS>(sa, t.pos + q, P, ubis, ubi, gs, hkf, cnt, sum, ntest);
+        count_pair<NT, SUMS>(sb, t.pos + q + 1, P, ubis, ubi, gs, hkf, cnt, sum, ntest);
+    }
+    if (q < gb) single(q);
+}
+
+// Exclusive scan of a[0 .. len) into b (block-wide; ends with a barrier).
+__device__ __forceinline__ void block_scan(const int* a, int* b, int len, int* s_w) {
+    const int per = (len + kJT - 1) / kJT;
+    const int b0 = threadIdx.x * per, b1 = min(b0 + per, len);
+    int sum = 0;
+    for (int i = b0; i < b1; i++) sum += a[i];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int tot;
+    const int ex = warp_excl_scan(sum, lane, tot);
+    if (lane == 0) s_w[w] = tot;
+    __syncthreads();
+    int base = 0;
+    for (int k = 0; k < w; k++) base += s_w[k];
+    int run = base + ex;
+    for (int i = b0; i < b1; i++) {
+        const int v = a[i];
+        b[i] = run;
+        run += v;
+    }
+    __syncthreads();
+}
+
+// Persistent CTAs, each taking one row of cells at a time (a counter).
+template <int NT, bool SUMS>
+__global__ void __launch_bounds__(kJT, kJoinMinBlocks)
+k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nrows,
+       int nhalo, BinInfo* __restrict__ info, const float4* __restrict__ packs,
+       const double* __restrict__ ubis, Header* __restrict__ Hp, const int* __restrict__ start,
+       const double* __restrict__ gs, const float4* __restrict__ g4, const JoinParams P,
+       int* __restrict__ counts, double* __restrict__ sums) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t* s_box = reinterpret_cast<uint64_t*>(smem);        // kBMax sorted boxes
+    float* s_gx = reinterpret_cast<float*>(s_box + kBMax);      // kGMax staged g
+    float* s_gy = s_gx + kGMax;
+    float* s_gz = s_gy + kGMax;
+    int* s_gp = reinterpret_cast<int*>(s_gz + kGMax);
+    const int nh1 = max(P.nxx, nhalo) + 1;
+    int* s_h = s_gp + kGMax;                                    // counts / cursors (nh1)
+    int* s_s = s_h + nh1;                                       // exclusive starts (nh1)
+    int* s_rp = s_s + nh1;                                      // halo rows: candidate prefix
+    int* s_rs = s_rp + (nhalo + 1);                             // halo rows: first g
+    __shared__ int s_row, s_w[kJW];
+    const Staged T{s_gx, s_gy, s_gz, s_gp};
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned ntest = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_row = atomicAdd(&info->next_row, 1);
+        __syncthreads();
+        const int r = s_row;
+        __syncthreads();
+        if (r >= nrows) break;
+        const int b0 = rstart[r], b1 = rstart[r + 1];
+        if (b0 == b1) continue;
+        const int iy = r % P.nx, iz = r / P.nx;
+        const float ylo = fmaf((float)iy, P.cs, P.rlo), yhi = fmaf((float)(iy + 1), P.cs, P.rhi);
+        const float zlo = fmaf((float)iz, P.cs, P.rlo), zhi = fmaf((float)(iz + 1), P.cs, P.rhi);
+        const int ry0 = max(iy - P.R, 0), rz0 = max(iz - P.R, 0);
+        const int ny = min(iy + P.R, P.nx - 1) - ry0 + 1;
+        const int nhr = ny * (min(iz + P.R, P.nx - 1) - rz0 + 1);
+        for (int p0 = b0; p0 < b1; p0 += kBMax) {
+            const int nb = min(kBMax, b1 - p0);
+            // the part's boxes sorted by x cell
+            for (int x = threadIdx.x; x <= P.nxx; x += kJT) s_h[x] = 0;
+            __syncthreads();
+            for (int i = threadIdx.x; i < nb; i += kJT) atomicAdd(s_h + box_fx(recs[p0 + i]), 1);
+            __syncthreads();
+            block_scan(s_h, s_s, P.nxx + 1, s_w);
+            for (int x = threadIdx.x; x <= P.nxx; x += kJT) s_h[x] = 0;
+            __syncthreads();
+            for (int i = threadIdx.x; i < nb; i += kJT) {
+                const uint64_t rec = recs[p0 + i];
+                const int fx = box_fx(rec);
+                s_box[s_s[fx] + atomicAdd(s_h + fx, 1)] = rec;
+            }
+            __syncthreads();
+            // x cells the part's boxes can reach, and the halo rows' g in them
+            const int fxa = max(box_fx(s_box[0]) - P.Rx, 0);
+            const int fxb = min(box_fx(s_box[nb - 1]) + P.Rx, P.nxx - 1);
+            const int gw = fxb - fxa + 1;
+            for (int j = threadIdx.x; j <= nhr; j += kJT) {
+                int len = 0;
+                if (j < nhr) {
+                    const int zq = j / ny;
+                    const int64_t base = ((int64_t)(rz0 + zq) * P.nx + (ry0 + j - zq * ny)) * P.nxx;
+                    const int st = start[base + fxa];
+                    s_rs[j] = st;
+                    len = start[base + fxb + 1] - st;
+                }
+                s_h[j] = len;
+            }
+            __syncthreads();
+            block_scan(s_h, s_rp, nhr + 1, s_w);
+            const int ncand = s_rp[nhr];
+            // tiles of at most kGMax staged g, each sorted by x cell
+            for (int c0 = 0; c0 < ncand;) {
+                for (int x = threadIdx.x; x <= gw; x += kJT) s_h[x] = 0;
+                __syncthreads();
+                // candidate q: its g (w: its x cell) and position; true when
+                // inside the row's y/z region
+                auto candidate = [&](int q, float4& v, int& pos) {
+                    int lo = 0, hi = nhr - 1;              // last halo row with s_rp <= q
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (s_rp[mid] <= q) lo = mid; else hi = mid - 1;
+                    }
+                    pos = s_rs[lo] + (q - s_rp[lo]);
+                    v = __ldg(g4 + pos);
+                    return v.y >= ylo && v.y <= yhi && v.z >= zlo && v.z <= zhi;
+                };
+                int cend = c0, tot = 0;
+                while (cend < ncand && tot <= kGMax - kJT) {
+                    const int q = cend + threadIdx.x;
+                    bool in = false;
+                    if (q < ncand) {
+                        float4 v;
+                        int pos;
+                        in = candidate(q, v, pos);
+                        if (in) atomicAdd(s_h + (__float_as_int(v.w) - fxa), 1);
+                    }
+                    tot += __syncthreads_count(in);
+                    cend = min(cend + kJT, ncand);
+                }
+                block_scan(s_h, s_s, gw + 1, s_w);
+                for (int x = threadIdx.x; x <= gw; x += kJT) s_h[x] = 0;
+                __syncthreads();
+                for (int q = c0 + threadIdx.x; q < cend; q += kJT) {
+                    float4 v;
+                    int pos;
+                    if (candidate(q, v, pos)) {
+                        const int cx = __float_as_int(v.w) - fxa;
+                        const int slot = s_s[cx] + atomicAdd(s_h + cx, 1);
+                        s_gx[slot] = v.x;
+                        s_gy[slot] = v.y;
+                        s_gz[slot] = v.z;
+                        s_gp[slot] = pos;
+                    }
+                }
+                __syncthreads();
+                // runs of 32 sorted boxes, one warp each
+                for (int k0 = 32 * w; k0 < nb; k0 += 32 * kJW) {
+                    const int nrun = min(32, nb - k0);
+                    const int ga = s_s[max(box_fx(s_box[k0]) - P.Rx, fxa) - fxa];
+                    const int gb = s_s[min(box_fx(s_box[k0 + nrun - 1]) + P.Rx, fxb) - fxa + 1];
+                    if (lane < nrun && ga < gb) {
+                        const uint64_t rec = s_box[k0 + lane];
+                        const int64_t ubi = P.i0 + (int64_t)(rec >> 40);
+                        const float hkf[3] = {(float)((int)((rec >> 31) & 511) - kHklOff),
+                                              (float)((int)((rec >> 22) & 511) - kHklOff),
+                                              (float)((int)((rec >> 13) & 511) - kHklOff)};
+                        const float4 p0 = __ldg(packs + 3 * ubi);
+                        const float4 p1 = __ldg(packs + 3 * ubi + 1);
+                        const float4 p2 = __ldg(packs + 3 * ubi + 2);
+                        const float u[9] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w, p2.x};
+                        uint64_t uu[9], hh[3];
+#pragma unroll
+                        for (int e = 0; e < 9; e++) uu[e] = pk2(u[e], u[e]);
+#pragma unroll
+                        for (int e = 0; e < 3; e++) hh[e] = pk2(hkf[e], hkf[e]);
+                        int cnt[NT];
+                        double sum[NT];
+#pragma unroll
+                        for (int j = 0; j < NT; j++) {
+                            cnt[j] = 0;
+                            sum[j] = 0.;
+                        }
+                        test_range<NT, SUMS>(T, ga, gb, u, uu, hh, hkf, P, ubis, ubi, gs, cnt, sum,
+                                             ntest);
+#pragma unroll
+                        for (int j = 0; j < NT; j++) {
+                            if (cnt[j]) atomicAdd(counts + ubi * NT + j, cnt[j]);
+                            if (SUMS && cnt[j]) atomicAdd(sums + ubi * NT + j, sum[j]);
+                        }
+                    }
+                }
+                __syncthreads();
+                c0 = cend;
+            }
+        }
+    }
+    const long long tt = warp_sum((long long)ntest);
+    if (lane == 0 && tt) atomicAdd(&Hp->ntested, (unsigned long long)tt);
+}
+
+// UBIs outside the binned path's limits: exact FP64 over every regular g, one
+// warp per (listed UBI, part).
+template <int NT, bool SUMS>
+__global__ void __launch_bounds__(kBT)
+k_fallback(const double* __restrict__ ubis, const int* __restrict__ list, int nlist,
+           Header* __restrict__ Hp, const int* __restrict__ start, const double* __restrict__ gs,
+           Tols tols, int* __restrict__ counts, double* __restrict__ sums) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wk = ((int64_t)blockIdx.x * kBT + threadIdx.x) >> 5;
+    if (wk >= (int64_t)nlist * kFallbackParts) return;  // uniform per warp
+    const int i = list[wk / kFallbackParts];
+    const int part = (int)(wk % kFallbackParts);
+    const int64_t nreg = start[Hp->ncells];
+    double u[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) u[e] = ubis[9 * (int64_t)i + e];
+    int cnt[NT];
+    double sum[NT];
+#pragma unroll
+    for (int j = 0; j < NT; j++) {
+        cnt[j] = 0;
+        sum[j] = 0.;
+    }
+    for (int64_t f = (int64_t)part * 32 + lane; f < nreg; f += 32 * (int64_t)kFallbackParts) {
+        double ih[3];
+        const double s = drlv2_exact(u, gs[3 * f], gs[3 * f + 1], gs[3 * f + 2], ih);
+#pragma unroll
+        for (int j = 0; j < NT; j++)
+            if (s < tols.t[j] * tols.t[j]) {
+                cnt[j]++;
+                sum[j] += s;
+            }
+    }
+#pragma unroll
+    for (int j = 0; j < NT; j++) {
+        const int c = warp_sum(cnt[j]);
+        const double sm = warp_sum(sum[j]);
+        if (lane == 0 && c) {
+            atomicAdd(counts + (int64_t)i * NT + j, c);
+            if (SUMS) atomicAdd(sums + (int64_t)i * NT + j, sm);
+        }
+    }
+    if (part == 0 && lane == 0) atomicAdd(&Hp->nfallback, 1ull);
+}
+
+// The g-vectors outside the regular range, for every UBI: one warp per UBI.
+template <int NT, bool SUMS>
+__global__ void __launch_bounds__(kBT)
+k_special(const double* __restrict__ ubis, int64_t m, const double* __restrict__ gv,
+          const int* __restrict__ special, const int* __restrict__ nspecial, Tols tols,
+          int* __restrict__ counts, double* __restrict__ sums) {
+    const int lane = threadIdx.x & 31;
+    const int64_t i = ((int64_t)blockIdx.x * kBT + threadIdx.x) >> 5;
+    if (i >= m) return;  // uniform per warp
+    const int ns = *nspecial;
+    double u[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
+    int cnt[NT];
+    double sum[NT];
+#pragma unroll
+    for (int j = 0; j < NT; j++) {
+        cnt[j] = 0;
+        sum[j] = 0.;
+    }
+    for (int q = lane; q < ns; q += 32) {
+        const int64_t k = special[q];
+        double ih[3];
+        const double s = drlv2_exact(u, gv[3 * k], gv[3 * k + 1], gv[3 * k + 2], ih);
+#pragma unroll
+        for (int j = 0; j < NT; j++)
+            if (s < tols.t[j] * tols.t[j]) {
+                cnt[j]++;
+                sum[j] += s;
+            }
+    }
+#pragma unroll
+    for (int j = 0; j < NT; j++) {
+        const int c = warp_sum(cnt[j]);
+        const double sm = warp_sum(sum[j]);
+        if (lane == 0 && c) {
+            atomicAdd(counts + i * NT + j, c);
+            if (SUMS) atomicAdd(sums + i * NT + j, sm);
+        }
+    }
+}
+
+template <int NT, bool SUMS>
+int launch_join(int grid, size_t smem, const uint64_t* recs, const int* rstart, int nrows,
+                int nhalo, BinInfo* info, const float4* packs, const double* ubis, Header* H,
+                const int* start, const double* gs, const float4* g4, const JoinParams& P,
+                int* counts, double* sums, cudaStream_t st) {
+    ID11B_CHECK(cudaFuncSetAttribute(k_join<NT, SUMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    k_join<NT, SUMS><<<grid, kJT, smem, st>>>(recs, rstart, nrows, nhalo, info, packs, ubis, H,
+                                              start, gs, g4, P, counts, sums);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+template <int NT, bool SUMS>
+int launch_rest(const double* ubis, int64_t m, const int* fallback, int nfallback, Header* H,
+                const int* start, const double* gs, const double* gv, const int* special,
+                const int* nspecial, int has_special, const Tols& T, int* counts, double* sums,
+                cudaStream_t st) {
+    if (nfallback > 0) {
+        const int64_t warps = (int64_t)nfallback * kFallbackParts;
+        k_fallback<NT, SUMS><<<(unsigned)((warps + kBW - 1) / kBW), kBT, 0, st>>>(
+            ubis, fallback, nfallback, H, start, gs, T, counts, sums);
+        ID11B_CHECK_LAUNCH();
+    }
+    if (has_special) {
+        k_special<NT, SUMS><<<(unsigned)((m + kBW - 1) / kBW), kBT, 0, st>>>(
+            ubis, m, gv, special, nspecial, T, counts, sums);
+        ID11B_CHECK_LAUNCH();
+    }
+    return ID11B_OK;
+}
+
+// resident CTAs per SM of a kernel with the given dynamic shared memory
+template <class K>
+int ctas_per_sm(K kernel, int threads, size_t smem) {
+    int per = 0;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) !=
+            cudaSuccess || per < 1)
+        per = 1;
+    return per;
+}
+
+template <int NT, bool SUMS>
+int join_ctas(size_t smem) { return ctas_per_sm(k_join<NT, SUMS>, kJT, smem); }
+
+// float nearest to x in the given direction (x itself when representable)
+float float_rd(double x) {
+    float f = (float)x;
+    if ((double)f > x) f = nextafterf(f, -INFINITY);
+    return f;
+}
+float float_ru(double x) {
+    float f = (float)x;
+    if ((double)f < x) f = nextafterf(f, INFINITY);
+    return f;
+}
+
+
+}  // namespace bins
+}  // namespace grid
+}  // namespace id11b
+
+using namespace id11b::grid;
+using namespace id11b::grid::bins;
+
+extern "C" int64_t id11b_grid_bins_workspace_bytes(int64_t m, int32_t nx, int32_t xsub,
+                                                   int64_t boxes) {
+    if (m < 0 || !grid_dims_ok(nx, xsub) || boxes < 0) return -1;
+    return (int64_t)bin_layout(m, (int64_t)nx * nx, boxes).bytes;
+}
+
+#define ID11B_BINS_DISPATCH(FN, ...)                                                        \
+    (sums ? (ntol == 1   ? FN<1, true>(__VA_ARGS__)                                         \
+             : ntol == 2 ? FN<2, true>(__VA_ARGS__)                                         \
+             : ntol == 3 ? FN<3, true>(__VA_ARGS__)                                         \
+                         : FN<4, true>(__VA_ARGS__))                                        \
+          : (ntol == 1   ? FN<1, false>(__VA_ARGS__)                                        \
+             : ntol == 2 ? FN<2, false>(__VA_ARGS__)                                        \
+             : ntol == 3 ? FN<3, false>(__VA_ARGS__)                                        \
+                         : FN<4, false>(__VA_ARGS__)))
+
+extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const double* gv,
+                                         int64_t n, int32_t nx, int32_t xsub,
+                                         const void* gridbuf, const double* tols_host, int ntol,
+                                         int32_t* counts, double* sums, void* ws,
+                                         int64_t ws_bytes, void* stream) {
+    if (!tols_host || ntol < 1 || ntol > ID11B_MAX_TOLS || m < 0 || n < 0 ||
+        !grid_dims_ok(nx, xsub) || !gridbuf || !ws || (m > 0 && (!ubis || !counts)) ||
+        (n > 0 && !gv))
+        return ID11B_ERR_ARG;
+    Tols T;
+    double tmax = 0.;
+    for (int j = 0; j < ID11B_MAX_TOLS; j++) T.t[j] = j < ntol ? tols_host[j] : 0.;
+    for (int j = 0; j < ntol; j++) {
+        if (!(tols_host[j] >= 0.) || !(tols_host[j] < kTolLimit)) return ID11B_ERR_ARG;
+        tmax = fmax(tmax, tols_host[j]);
+    }
+    if (((uintptr_t)gridbuf & 255) || ((uintptr_t)ws & 255)) return ID11B_ERR_ALIGN;
+    if (m > INT32_MAX - 1) return ID11B_ERR_SIZE;
+    const int nrows = nx * nx;
+    const int nxx = nx * xsub;
+    if (nrows > kMaxRows || nxx > kMaxNxx) return ID11B_ERR_SIZE;  // use id11b_dev_score_grid
+    // the largest box capacity the workspace holds
+    const BinLayout L0 = bin_layout(m, nrows, 0);
+    if (ws_bytes < (int64_t)L0.bytes) return ID11B_ERR_SIZE;
+    int64_t cap = (ws_bytes - (int64_t)L0.bytes) / (int64_t)sizeof(uint64_t);
+    while (cap > 0 && (int64_t)bin_layout(m, nrows, cap).bytes > ws_bytes) cap -= 1 + cap / 1024;
+    if (cap > INT32_MAX - 1) cap = INT32_MAX - 1;
+    const BinLayout B = bin_layout(m, nrows, cap);
+    cudaStream_t st = (cudaStream_t)stream;
+    const Layout L = layout(n, (int64_t)nrows * nxx);
+    char* g = (char*)gridbuf;
+    Header* H = (Header*)g;
+    const int* start = (const int*)(g + L.start);
+    const double* gs = (const double*)(g + L.g);
+    const float4* g4 = (const float4*)(g + L.g4);
+    char* w = (char*)ws;
+    BinInfo* info = (BinInfo*)(w + B.info);
+    float4* packs = (float4*)(w + B.packs);
+    int* cnt_ubi = (int*)(w + B.cnt_ubi);
+    int* fallback = (int*)(w + B.fallback);
+    int* cta_rows = (int*)(w + B.cta_rows);
+    int* rowtot = (int*)(w + B.rowtot);
+    int* rstart = (int*)(w + B.rstart);
+    int* tot = (int*)(w + B.tot);
+    uint64_t* recs = (uint64_t*)(w + B.recs);
+    ID11B_CHECK(cudaMemsetAsync(&H->nfallback, 0, 2 * sizeof(unsigned long long), st));
+    if (m == 0) return ID11B_OK;
+    ID11B_CHECK(cudaMemsetAsync(counts, 0, sizeof(int32_t) * (size_t)(m * ntol), st));
+    if (sums) ID11B_CHECK(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)(m * ntol), st));
+    ID11B_CHECK(cudaMemsetAsync(info, 0, sizeof(BinInfo), st));
+    // the enumeration's CTAs (same count and UBI ranges in both passes)
+    const size_t esmem = sizeof(int) * (size_t)nrows;
+    static thread_local int enum_per_sm = 0;
+    if (!enum_per_sm) enum_per_sm = ctas_per_sm(k_enum, kET, 64 * 1024);
+    ID11B_CHECK(cudaFuncSetAttribute(k_enum, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)esmem));
+    const int nctas = (int)std::min<int64_t>(kMaxEnumCtas, (int64_t)num_sms() * enum_per_sm);
+    auto enumerate = [&](int mode, int64_t i0, int64_t mc, int first) {
+        const int64_t per = (mc + nctas - 1) / nctas;
+        const int grid = (int)std::min<int64_t>(nctas, (mc + per - 1) / per);
+        k_enum<<<grid, kET, esmem, st>>>(mode, ubis, i0, mc, per, H, start, tmax, first, nrows,
+                                         info, packs, cnt_ubi, fallback, cta_rows, rstart, recs);
+        return grid;
+    };
+    int egrid = enumerate(0, 0, m, 1);
+    ID11B_CHECK_LAUNCH();
+    // small reads back to the host: the box total (for the capacity), the
+    // band's inputs, the grid header and the number of g outside the regular range
+    BinInfo bi;
+    Header hh;
+    int nspecial = 0;
+    ID11B_CHECK(cudaMemcpyAsync(&bi, info, sizeof(BinInfo), cudaMemcpyDeviceToHost, st));
+    ID11B_CHECK(cudaMemcpyAsync(&hh, H, sizeof(Header), cudaMemcpyDeviceToHost, st));
+    ID11B_CHECK(cudaMemcpyAsync(&nspecial, g + L.spos + sizeof(int) * (size_t)n, sizeof(int),
+                                cudaMemcpyDeviceToHost, st));
+    ID11B_CHECK(cudaStreamSynchronize(st));
+    // UBI ranges whose boxes fit the capacity and whose indices fit a record
+    std::vector<int64_t> cuts{0};
+    if ((int64_t)bi.total > cap || m > (int64_t(1) << kUbiBits)) {
+        std::vector<int> cu((size_t)m);
+        ID11B_CHECK(cudaMemcpyAsync(cu.data(), cnt_ubi, sizeof(int) * (size_t)m,
+                                    cudaMemcpyDeviceToHost, st));
+        ID11B_CHECK(cudaStreamSynchronize(st));
+        int64_t acc = 0;
+        for (int64_t i = 0; i < m; i++) {
+            if (cu[i] > cap) return ID11B_ERR_SIZE;
+            if (acc + cu[i] > cap || i - cuts.back() >= (int64_t(1) << kUbiBits)) {
+                cuts.push_back(i);
+                acc = 0;
+            }
+            acc += cu[i];
+        }
+    }
+    cuts.push_back(m);
+    // the screening kernel's band (score_batch.cu) for gmax = G and the largest
+    // row sum of the binned UBIs; the region geometry
+    JoinParams P;
+    {
+        const double G = -hh.lo;
+        float smax;
+        memcpy(&smax, &bi.smax_bits, sizeof(smax));
+        const double E = 6.0 * kEps32 * (double)smax * G;
+        P.hmax = 0.f;
+        for (int j = 0; j < ID11B_MAX_TOLS; j++) {
+            const double t = T.t[j], TT = t * t;
+            const double band = 1.25 * (3.0 * E * (2.0 * (t + 1e-3) + E) +
+                                        4.0 * kEps32 * (TT + 0.01));
+            P.lo[j] = float_rd(TT - band);
+            P.hi[j] = float_ru(TT + band);
+            P.t2[j] = TT;
+            if (j < ntol) P.hmax = fmaxf(P.hmax, P.hi[j]);
+        }
+        double W;
+        memcpy(&W, &bi.wmax_bits, sizeof(W));
+        // eps: far above the FP32 rounding of the box centres' cells (about
+        // 2^-23 of |c| + |lo|) and of the FP32 region bounds
+        const double eps = 2e-5 * (1. + G);
+        const double csx = 1.0 / hh.inv_csx;
+        P.rlo = float_rd(hh.lo - W - eps);
+        P.rhi = float_ru(hh.lo + W + eps);
+        P.cs = (float)hh.cs;
+        P.R = (int)ceil((W + 2. * eps) / hh.cs);
+        P.Rx = (int)ceil((W + 2. * eps) / csx);
+        P.nx = hh.nx;
+        P.nxx = hh.nxx;
+    }
+    const int nhalo = (2 * P.R + 1) * (2 * P.R + 1);
+    if (bi.total > 0 && nhalo > kMaxHalo) return ID11B_ERR_SIZE;  // cells far smaller than W
+    const size_t jsmem = sizeof(uint64_t) * kBMax + 4 * sizeof(float) * kGMax +
+                         2 * sizeof(int) * (size_t)(std::max(nxx, nhalo) + 1) +
+                         2 * sizeof(int) * (size_t)(nhalo + 1);
+    const int jgrid = num_sms() * ID11B_BINS_DISPATCH(join_ctas, jsmem);
+    for (size_t c = 0; c + 1 < cuts.size() && bi.total > 0; c++) {
+        const int64_t i0 = cuts[c], mc = cuts[c + 1] - cuts[c];
+        if (cuts.size() > 2) {
+            egrid = enumerate(0, i0, mc, 0);
+            ID11B_CHECK_LAUNCH();
+        }
+        k_row_offsets<<<grid_for((int64_t)nrows * 32, kGT), kGT, 0, st>>>(cta_rows, egrid, nrows,
+                                                                         rowtot);
+        ID11B_CHECK_LAUNCH();
+        ID11B_CHECK(cudaMemsetAsync(rowtot + nrows, 0, sizeof(int), st));
+        int rc = scan(rowtot, nrows + 1, rstart, tot, st);
+        if (rc) return rc;
+        enumerate(1, i0, mc, 0);
+        ID11B_CHECK_LAUNCH();
+        ID11B_CHECK(cudaMemsetAsync(&info->next_row, 0, sizeof(int), st));
+        P.i0 = i0;
+        rc = ID11B_BINS_DISPATCH(launch_join, jgrid, jsmem, recs, rstart, nrows, nhalo, info,
+                                 packs, ubis, H, start, gs, g4, P, counts, sums, st);
+        if (rc) return rc;
+    }
+    return ID11B_BINS_DISPATCH(launch_rest, ubis, m, fallback, bi.nfallback, H, start, gs, gv,
+                               (const int*)(g + L.spec), (const int*)(g + L.spos) + n,
+                               nspecial > 0, T, counts, sums, st);
+}

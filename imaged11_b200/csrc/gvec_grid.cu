@@ -23,16 +23,11 @@
 // singular, ill-conditioned, or with more candidate hkl than g-vectors) are
 // scored by a plain scan of every regular g; g-vectors outside the regular
 // range (non-finite or |g_j| > 1024) by a scan over that list.
-#include <math.h>
-#include <limits.h>
-#include <stdint.h>
-
-#include "common.cuh"
+#include "grid.cuh"
 
 namespace id11b {
 namespace grid {
 
-constexpr int kGT = 256;           // threads per CTA of the build kernels
 // scoring CTAs: warps (one per work item) and the resident CTAs per SM the
 // register budget is compiled for.  Occupancy decides the speed of the
 // latency-bound lookups: 20,000 UBIs x 1.1M g on B200 took 13.0 ms at 8 warps
@@ -46,79 +41,6 @@ constexpr int kGT = 256;           // threads per CTA of the build kernels
 #endif
 constexpr int kSW = ID11B_GRID_WARPS;
 constexpr int kST = 32 * kSW;
-constexpr int kScanT = 1024;       // scan CTA
-constexpr int kScanPer = 4 * kScanT;
-constexpr double kGLimit = 1024.0;  // regular g: finite, every |g_j| <= 1024
-constexpr double kHklMargin = 1e-6;
-constexpr double kMaxCond = 1e6;
-constexpr int kMaxParts = 64;
-
-struct Header {
-    double lo, cs, inv_cs;  // cube [lo, lo + nx*cs)^3; y and z cells of side cs
-    double inv_csx;         // x cells: side cs / xsub (nxx = nx * xsub of them)
-    double rmax;            // max |g| over regular g (rounded up)
-    int64_t ncells;
-    int64_t n;
-    int32_t nx;
-    int32_t nxx;
-    unsigned long long nfallback;  // UBIs scored by the plain scan (last call)
-    unsigned long long ntested;    // (UBI, g) pairs evaluated in FP64 (last call)
-};
-
-struct Tols {
-    double t[ID11B_MAX_TOLS];
-};
-
-__host__ __device__ inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
-
-// Grid buffer: header | cnt[ncells+1] | start[ncells+1] | g[n][3] | gidx[n] |
-// flag[n+1] | spos[n+1] | spec[n] | scan totals
-struct Layout {
-    size_t header, cnt, start, g, idx, flag, spos, spec, tot, bytes;
-};
-
-__host__ __device__ inline Layout layout(int64_t n, int64_t ncells) {
-    Layout L;
-    const size_t nn = (size_t)(n > 0 ? n : 1);
-    const int64_t big = ncells + 1 > n + 1 ? ncells + 1 : n + 1;
-    size_t o = 0;
-    L.header = o; o = al256(o + sizeof(Header));
-    L.cnt = o;    o = al256(o + sizeof(int) * (size_t)(ncells + 1));
-    L.start = o;  o = al256(o + sizeof(int) * (size_t)(ncells + 1));
-    L.g = o;      o = al256(o + sizeof(double) * 3 * nn);
-    L.idx = o;    o = al256(o + sizeof(int) * nn);
-    L.flag = o;   o = al256(o + sizeof(int) * (nn + 1));
-    L.spos = o;   o = al256(o + sizeof(int) * (nn + 1));
-    L.spec = o;   o = al256(o + sizeof(int) * nn);
-    L.tot = o;    o = al256(o + sizeof(int) * (size_t)((big + kScanPer - 1) / kScanPer + 1));
-    L.bytes = o;
-    return L;
-}
-
-__device__ __forceinline__ bool regular(double a, double b, double c) {
-    double m = fmax(fabs(a), fmax(fabs(b), fabs(c)));
-    return isfinite(a) && isfinite(b) && isfinite(c) && m <= kGLimit;
-}
-
-// Monotone in x (RN subtraction and multiplication by a positive constant,
-// clamp, truncation of a non-negative value); NaN must not reach it.
-__device__ __forceinline__ int coord(double x, const Header& H) {
-    double f = __dmul_rn(__dsub_rn(x, H.lo), H.inv_cs);
-    f = fmin(fmax(f, 0.0), (double)(H.nx - 1));
-    return (int)f;
-}
-
-// x is cut finer (a row of cells is one contiguous range whatever its length,
-// so finer x cells cost memory, not lookups)
-__device__ __forceinline__ int coord_x(double x, const Header& H) {
-    double f = __dmul_rn(__dsub_rn(x, H.lo), H.inv_csx);
-    f = fmin(fmax(f, 0.0), (double)(H.nxx - 1));
-    return (int)f;
-}
-
-__device__ __forceinline__ int64_t cell_of(double a, double b, double c, const Header& H) {
-    return ((int64_t)coord(c, H) * H.nx + coord(b, H)) * H.nxx + coord_x(a, H);
-}
 
 // ------------------------------------------------------------------ build --
 // max |g_j| and max |g| over regular g, as float bits rounded up
@@ -290,63 +212,18 @@ k_sort_cells(const int* __restrict__ start, int64_t ncells, double* __restrict__
     }
 }
 
-// ------------------------------------------------------------- per UBI ----
-// Query plan of one UBI (uniform across the warp).
-struct Plan {
-    double ub[9];      // UBI^-1
-    double w[3];       // box half-widths
-    int64_t lo[3];     // hkl box
-    int64_t nh[3];
-    bool ok;           // false: plain scan of every regular g
-};
-
-__device__ __forceinline__ Plan make_plan(const double u[9], double tmax, const Header& H,
-                                          int64_t nreg) {
-    Plan P;
-    bool ok = true;
-#pragma unroll
-    for (int e = 0; e < 9; e++) ok = ok && isfinite(u[e]);
-    const double c00 = u[4] * u[8] - u[5] * u[7], c01 = u[5] * u[6] - u[3] * u[8],
-                 c02 = u[3] * u[7] - u[4] * u[6];
-    const double det = u[0] * c00 + u[1] * c01 + u[2] * c02;
-    ok = ok && isfinite(det) && det != 0.;
-    const double id = 1.0 / det;
-    P.ub[0] = c00 * id;
-    P.ub[1] = (u[2] * u[7] - u[1] * u[8]) * id;
-    P.ub[2] = (u[1] * u[5] - u[2] * u[4]) * id;
-    P.ub[3] = c01 * id;
-    P.ub[4] = (u[0] * u[8] - u[2] * u[6]) * id;
-    P.ub[5] = (u[2] * u[3] - u[0] * u[5]) * id;
-    P.ub[6] = c02 * id;
-    P.ub[7] = (u[1] * u[6] - u[0] * u[7]) * id;
-    P.ub[8] = (u[0] * u[4] - u[1] * u[3]) * id;
-    double nu = 0., nb = 0.;
-#pragma unroll
-    for (int e = 0; e < 9; e++) {
-        nu += u[e] * u[e];
-        nb += P.ub[e] * P.ub[e];
-        ok = ok && isfinite(P.ub[e]);
-    }
-    ok = ok && sqrt(nu) * sqrt(nb) <= kMaxCond;
-    const double G = -H.lo;  // every regular g lies in [-G, G]^3
-    double total = 1.;
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-        const double s = fabs(u[3 * r]) + fabs(u[3 * r + 1]) + fabs(u[3 * r + 2]);
-        const double hm = s * G + 1.0;
-        ok = ok && hm < 1e6;
-        const double l = floor(-hm), h = ceil(hm);
-        P.lo[r] = ok ? (int64_t)l : 0;
-        P.nh[r] = ok ? (int64_t)(h - l) + 1 : 1;
-        total *= (h - l) + 1.;
-        P.w[r] = (tmax + kHklMargin) *
-                 sqrt(P.ub[3 * r] * P.ub[3 * r] + P.ub[3 * r + 1] * P.ub[3 * r + 1] +
-                      P.ub[3 * r + 2] * P.ub[3 * r + 2]) * (1. + 1e-9);
-        ok = ok && isfinite(P.w[r]);
-    }
-    ok = ok && total <= (double)nreg;  // more candidate hkl than g: the plain scan is cheaper
-    P.ok = ok;
-    return P;
+// FP32 (round to nearest) copy of the cell-sorted regular g, for staging,
+// with the g's x cell (as int bits) in w
+__global__ void __launch_bounds__(kGT)
+k_sorted_f32(const int* __restrict__ start, const Header* __restrict__ Hp,
+             const double* __restrict__ gs, float4* __restrict__ g4) {
+    const Header H = *Hp;
+    const int64_t nreg = start[H.ncells];
+    for (int64_t p = (int64_t)blockIdx.x * kGT + threadIdx.x; p < nreg;
+         p += (int64_t)gridDim.x * kGT)
+        g4[p] = make_float4(__double2float_rn(gs[3 * p]), __double2float_rn(gs[3 * p + 1]),
+                            __double2float_rn(gs[3 * p + 2]),
+                            __int_as_float(coord_x(gs[3 * p], H)));
 }
 
 // Per-warp queue of hkl that reach the data.  Enumeration: 32 (h, k) columns
@@ -357,45 +234,6 @@ __device__ __forceinline__ Plan make_plan(const double u[9], double tmax, const 
 // queued the warp runs the 32 lookups together (lookup_batch).  The UBI's plan
 // lives in shared memory, not in registers.
 constexpr int kQueue = 64;
-
-struct WarpPlan {
-    double u[9], ub[9], w[3];
-    int lo[3], nh[3];
-};
-
-__device__ __forceinline__ unsigned long long pack_hkl(int h, int k, int l) {
-    return ((unsigned long long)(unsigned)(h + (1 << 20)) << 42) |
-           ((unsigned long long)(unsigned)(k + (1 << 20)) << 21) |
-           (unsigned long long)(unsigned)(l + (1 << 20));
-}
-
-__device__ __forceinline__ void unpack_hkl(unsigned long long q, double hkl[3]) {
-    hkl[0] = (double)((int)((q >> 42) & 0x1fffff) - (1 << 20));
-    hkl[1] = (double)((int)((q >> 21) & 0x1fffff) - (1 << 20));
-    hkl[2] = (double)((int)(q & 0x1fffff) - (1 << 20));
-}
-
-// Largest lane j with excl_j <= f, excl non-decreasing over lanes, excl_0 = 0.
-__device__ __forceinline__ int owner(int excl, int f) {
-    int j = 0;
-#pragma unroll
-    for (int st = 16; st > 0; st >>= 1) {
-        const int v = __shfl_sync(0xffffffffu, excl, j + st);
-        if (v <= f) j += st;
-    }
-    return j;
-}
-
-__device__ __forceinline__ int warp_excl_scan(int v, int lane, int& total) {
-    int incl = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    total = __shfl_sync(0xffffffffu, incl, 31);
-    return incl - v;
-}
 
 // Per-warp scratch for one batch of up to 32 lookups.
 struct Batch {
@@ -531,32 +369,6 @@ __device__ __forceinline__ void lookup_batch(const volatile WarpPlan* wp, Batch*
     __syncwarp();
 }
 
-// Plan of UBI i into the warp's shared slot; false: plain scan instead.
-__device__ __forceinline__ bool setup_plan(volatile WarpPlan* wp, const double* __restrict__ ubis,
-                                           int64_t i, double tmax, const Header& H,
-                                           int64_t nreg, int lane) {
-    double u[9];
-#pragma unroll
-    for (int e = 0; e < 9; e++) u[e] = ubis[9 * i + e];
-    const Plan P = make_plan(u, tmax, H, nreg);
-    const bool ok = P.ok && P.nh[0] < (1 << 20) && P.nh[1] < (1 << 20) && P.nh[2] < (1 << 20);
-    if (lane == 0) {
-#pragma unroll
-        for (int e = 0; e < 9; e++) {
-            wp->u[e] = u[e];
-            wp->ub[e] = P.ub[e];
-        }
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-            wp->w[r] = P.w[r];
-            wp->lo[r] = ok ? (int)P.lo[r] : 0;
-            wp->nh[r] = ok ? (int)P.nh[r] : 0;
-        }
-    }
-    __syncwarp();
-    return ok;
-}
-
 // Every (UBI, g) pair of work item `part` of `parts` whose drlv2 can be below
 // the plan's tolerance goes to act(pos, drlv2, own, g, ih): through the hkl lookup
 // when ok, else by a plain scan of the regular g (own = true: each g once).
@@ -581,75 +393,23 @@ __device__ __forceinline__ void walk(volatile WarpPlan* wp, Batch* bt, unsigned 
     if (lane == 0) bt->cn = 0;
     __syncwarp();
     const unsigned lt = (1u << lane) - 1u;
-    const int nh0 = wp->nh[0];
-    const int64_t nhk = (int64_t)nh0 * wp->nh[1];
-    for (int64_t hb = (int64_t)part * 32; hb < nhk; hb += 32 * (int64_t)parts) {
-        const int64_t hk = hb + lane;
-        int len = 0, l0 = 0, h = 0, k = 0;
-        if (hk < nhk) {
-            h = wp->lo[0] + (int)(hk % nh0);
-            k = wp->lo[1] + (int)(hk / nh0);
-            const double bx = wp->ub[2], by = wp->ub[5], bz = wp->ub[8];  // l direction
-            const double bb = bx * bx + by * by + bz * bz;
-            const double R = (H.rmax + sqrt(wp->w[0] * wp->w[0] + wp->w[1] * wp->w[1] +
-                                            wp->w[2] * wp->w[2])) * (1. + 1e-9) + 1e-12;
-            const double ax = wp->ub[0] * h + wp->ub[1] * k, ay = wp->ub[3] * h + wp->ub[4] * k,
-                         az = wp->ub[6] * h + wp->ub[7] * k;
-            const double ab = ax * bx + ay * by + az * bz;
-            const double aa = ax * ax + ay * ay + az * az;
-            const double disc = ab * ab - bb * (aa - R * R);
-            if (disc >= 0.) {
-                const double sq = sqrt(disc);
-                const double la = fmax(floor((-ab - sq) / bb) - 1., (double)wp->lo[2]);
-                const double lb = fmin(ceil((-ab + sq) / bb) + 1.,
-                                       (double)(wp->lo[2] + wp->nh[2] - 1));
-                if (la <= lb) {
-                    l0 = (int)la;
-                    len = (int)(lb - la) + 1;
-                }
-            }
-        }
-        int total;
-        const int excl = warp_excl_scan(len, lane, total);
-        for (int f0 = 0; f0 < total; f0 += 32) {
-            const int f = f0 + lane;
-            const int j = owner(excl, f);
-            const int hj = __shfl_sync(0xffffffffu, h, j);
-            const int kj = __shfl_sync(0xffffffffu, k, j);
-            const int lj = __shfl_sync(0xffffffffu, l0, j) + f - __shfl_sync(0xffffffffu, excl, j);
-            bool pass = false;
-            if (f < total) {
-                const double hkl[3] = {(double)hj, (double)kj, (double)lj};
-                bool in = true;
-                double d2 = 0.;
-                const double G = -H.lo;
-#pragma unroll
-                for (int r = 0; r < 3; r++) {
-                    const double c = wp->ub[3 * r] * hkl[0] + wp->ub[3 * r + 1] * hkl[1] +
-                                     wp->ub[3 * r + 2] * hkl[2];
-                    const double wr = wp->w[r];
-                    in = in && (c - wr <= G) && (c + wr >= -G);
-                    const double e = fmax(fabs(c) - wr, 0.);
-                    d2 += e * e;
-                }
-                pass = in && d2 <= H.rmax * H.rmax * (1. + 1e-9);
-            }
-            const unsigned mask = __ballot_sync(0xffffffffu, pass);
-            if (pass) q_w[qn + __popc(mask & lt)] = pack_hkl(hj, kj, lj);
-            qn += __popc(mask);
+    auto queue = [&](bool pass, int hj, int kj, int lj, const double*) {
+        const unsigned mask = __ballot_sync(0xffffffffu, pass);
+        if (pass) q_w[qn + __popc(mask & lt)] = pack_hkl(hj, kj, lj);
+        qn += __popc(mask);
+        __syncwarp();
+        if (qn >= 32) {
+            lookup_batch(wp, bt, q_w, 32, lane, H, start, gs, act);
+            const int rest = qn - 32;
+            unsigned long long v = 0;
+            if (lane < rest) v = q_w[32 + lane];
             __syncwarp();
-            if (qn >= 32) {
-                lookup_batch(wp, bt, q_w, 32, lane, H, start, gs, act);
-                const int rest = qn - 32;
-                unsigned long long v = 0;
-                if (lane < rest) v = q_w[32 + lane];
-                __syncwarp();
-                if (lane < rest) q_w[lane] = v;
-                __syncwarp();
-                qn = rest;
-            }
+            if (lane < rest) q_w[lane] = v;
+            __syncwarp();
+            qn = rest;
         }
-    }
+    };
+    enumerate_boxes(wp, part, parts, lane, H, queue);
     if (qn > 0) lookup_batch(wp, bt, q_w, qn, lane, H, start, gs, act);
     const int cn = bt->cn;
     if (cn > 0) eval_candidates(wp, bt, cn, lane, act);
@@ -1008,14 +768,14 @@ k_assign_special(const double* __restrict__ ubis, int64_t m, const double* __res
 namespace id11b {
 namespace grid {
 
-static int num_sms() {
+int num_sms() {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return sms > 0 ? sms : 148;
 }
 
-static unsigned grid_for(int64_t items, int per) {
+unsigned grid_for(int64_t items, int per) {
     int64_t b = (items + per - 1) / per;
     int64_t cap = (int64_t)num_sms() * 8;
     if (b > cap) b = cap;
@@ -1023,7 +783,7 @@ static unsigned grid_for(int64_t items, int per) {
 }
 
 // exclusive scan of x[0..len) into y (len >= 1), tot: scratch
-static int scan(const int* x, int64_t len, int* y, int* tot, cudaStream_t st) {
+int scan(const int* x, int64_t len, int* y, int* tot, cudaStream_t st) {
     const int64_t nb = (len + kScanPer - 1) / kScanPer;
     k_scan_local<<<(unsigned)nb, kScanT, 0, st>>>(x, len, y, tot);
     ID11B_CHECK_LAUNCH();
@@ -1035,7 +795,7 @@ static int scan(const int* x, int64_t len, int* y, int* tot, cudaStream_t st) {
 }
 
 // work items (warps) per UBI: enough warps for ~4 waves of 8 warps x 8 CTAs per SM
-static int score_parts(int64_t m) {
+int score_parts(int64_t m) {
     if (m <= 0) return 1;
     int64_t want = (int64_t)num_sms() * 64 * 4;
     int64_t p = (want + m - 1) / m;
@@ -1073,9 +833,13 @@ extern "C" int id11b_grid_plan(float gmax, int64_t n, double cell, int32_t* nx, 
     return ID11B_OK;
 }
 
-static bool grid_dims_ok(int32_t nx, int32_t xsub) {
+namespace id11b {
+namespace grid {
+bool grid_dims_ok(int32_t nx, int32_t xsub) {
     return nx >= 1 && nx <= 400 && xsub >= 1 && xsub <= 16 && (int64_t)nx * nx * nx * xsub <= (1 << 26);
 }
+}  // namespace grid
+}  // namespace id11b
 
 extern "C" int64_t id11b_grid_bytes(int64_t n, int32_t nx, int32_t xsub) {
     if (n < 0 || !grid_dims_ok(nx, xsub)) return -1;
@@ -1133,6 +897,9 @@ extern "C" int id11b_dev_build_grid(const double* gv, int64_t n, float gmax, flo
         ID11B_CHECK_LAUNCH();
         k_sort_cells<<<grid_for(ncells, kGT), kGT, 0, st>>>(start, ncells, (double*)(b + L.g),
                                                             (int*)(b + L.idx));
+        ID11B_CHECK_LAUNCH();
+        k_sorted_f32<<<grid_for(n, kGT), kGT, 0, st>>>(start, H, (const double*)(b + L.g),
+                                                       (float4*)(b + L.g4));
         ID11B_CHECK_LAUNCH();
     }
     return ID11B_OK;

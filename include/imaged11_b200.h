@@ -269,6 +269,30 @@ int id11b_dev_score_grid(const double *ubis, int64_t m, const double *gv, int64_
 int id11b_grid_stats(const void *gridbuf, int64_t *nregular, int64_t *nspecial,
                      int64_t *nfallback, int64_t *ntested, void *stream);
 
+/* The same counts (and optional FP64 sums of the counted drlv2) as
+ * id11b_dev_score_grid -- identical to the reference's score() for every
+ * (UBI, tol), ImageD11 src/closest.c:227-248 -- by a spatial join instead of
+ * per-box lookups: every (UBI, hkl) box that can reach the data is enumerated
+ * once, the boxes are sorted by the grid cell holding their centre, and each
+ * run of 32 boxes along a row of cells is tested against the g-vectors of
+ * its region (the cells it spans widened by the largest box half width),
+ * staged in shared memory, with the FP32 screening arithmetic; pairs inside
+ * the proven error band are re-evaluated with the reference's FP64
+ * arithmetic.  Tolerances must lie in [0, 0.4) (else ID11B_ERR_ARG: use
+ * id11b_dev_score_grid).  The workspace (256-byte aligned) holds per-UBI,
+ * per-cell and per-row tables plus 8.5 bytes per box:
+ * id11b_grid_bins_workspace_bytes(m, nx, xsub, boxes) for a box capacity;
+ * with fewer bytes than the call needs, the UBIs are processed in ranges that
+ * fit (ID11B_ERR_SIZE when one UBI's boxes alone do not fit).  The call reads
+ * the box total back to the host (one stream synchronisation).  Sums, when
+ * asked for, are added with double atomics: their last bits can differ
+ * between runs; counts never do. */
+int64_t id11b_grid_bins_workspace_bytes(int64_t m, int32_t nx, int32_t xsub, int64_t boxes);
+int id11b_dev_score_grid_bins(const double *ubis, int64_t m, const double *gv, int64_t n,
+                              int32_t nx, int32_t xsub, const void *gridbuf,
+                              const double *tols_host, int ntol, int32_t *counts, double *sums,
+                              void *ws, int64_t ws_bytes, void *stream);
+
 /* id11b_dev_score_and_assign_grid in pieces, for grains sharded over ranks
  * (one process per GPU): each rank runs pass -1 (reset of best (n uint64) and
  * lab (n int32)) and pass 0 over its share ubis[base : base+m]; best is

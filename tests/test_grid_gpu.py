@@ -1,9 +1,10 @@
 """Scoring through the reciprocal-space cell index vs the oracle and the
-golden vectors.
+golden vectors, by both methods: per-box lookups ("walk", every candidate
+pair evaluated in the reference's FP64 arithmetic) and the binned join
+("bins", FP32 screening with the proven FP64 recheck band).
 
-Counts are bit-exact: every candidate pair is evaluated in the reference's
-FP64 arithmetic and the lookup boxes are conservative, so the counted set is
-the reference's.  Sums of drlv2 are FP64 sums in another order than the
+Counts are bit-exact: the lookup boxes are conservative, so the counted set
+is the reference's.  Sums of drlv2 are FP64 sums in another order than the
 reference's loop: 1e-12 relative."""
 import numpy as np
 import pytest
@@ -11,6 +12,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 SUM_RTOL = 1e-12
+METHODS = ["walk", "bins"]
 
 
 @pytest.fixture(scope="module")
@@ -28,29 +30,32 @@ def scene():
     return ps, ubis
 
 
-def test_golden_counts(B, golden, cuda):
+@pytest.mark.parametrize("method", METHODS)
+def test_golden_counts(B, golden, method, cuda):
     d = golden["scoring"]
     grid = B.GvecGrid(d["sc_gv"])
-    c = B.score_grid(d["sc_ubis"], grid, d["sc_tols"]).cpu().numpy()
+    c = B.score_grid(d["sc_ubis"], grid, d["sc_tols"], method=method).cpu().numpy()
     assert np.array_equal(c, d["sc_counts"])
 
 
-def test_adversarial_and_special_g(B, golden, oracle, cuda):
+@pytest.mark.parametrize("method", METHODS)
+def test_adversarial_and_special_g(B, golden, oracle, method, cuda):
     d = golden["scoring"]
     grid = B.GvecGrid(d["adv_gv"])
     st = grid.stats()
     assert st["regular"] + st["special"] == len(d["adv_gv"])
     ubis = np.concatenate([d["adv_ubi"][None], d["sc_ubis"][:7]])
-    c = B.score_grid(ubis, grid, d["sc_tols"]).cpu().numpy()
+    c = B.score_grid(ubis, grid, d["sc_tols"], method=method).cpu().numpy()
     assert np.array_equal(c[0], d["adv_counts"])
     assert np.array_equal(c, oracle.score_many(ubis, d["adv_gv"], d["sc_tols"]))
 
 
-def test_scene_counts_and_sums(B, oracle, scene, cuda):
+@pytest.mark.parametrize("method", METHODS)
+def test_scene_counts_and_sums(B, oracle, scene, method, cuda):
     ps, ubis = scene
     tols = [0.02, 0.05, 0.1]
     grid = B.GvecGrid(ps.gv)
-    c, s = B.score_grid(ubis, grid, tols, sums=True)
+    c, s = B.score_grid(ubis, grid, tols, sums=True, method=method)
     c = c.cpu().numpy()
     s = s.cpu().numpy()
     assert np.array_equal(c, oracle.score_many(ubis, ps.gv, tols))
@@ -62,35 +67,46 @@ def test_scene_counts_and_sums(B, oracle, scene, cuda):
             n, mean, _ = oracle.score_and_refine(ubis[i], ps.gv, t)
             assert n == c[i, j]
             assert abs(s[i, j] - mean * n) <= SUM_RTOL * mean * n + 1e-300
-    # deterministic: the same sums bit for bit
-    c2, s2 = B.score_grid(ubis, grid, tols, sums=True)
-    assert np.array_equal(s2.cpu().numpy(), s)
+    c2, s2 = B.score_grid(ubis, grid, tols, sums=True, method=method)
+    assert np.array_equal(c2.cpu().numpy(), c)
+    if method == "walk":        # fixed-order sums: the same bits
+        assert np.array_equal(s2.cpu().numpy(), s)
+    else:                       # atomics: the same values to rounding
+        assert np.allclose(s2.cpu().numpy(), s, rtol=SUM_RTOL, atol=0)
 
 
+@pytest.mark.parametrize("method", METHODS)
 @pytest.mark.parametrize("cell,xsub", [(0.004, 4), (0.03, 1), (0.03, 16), (0.25, 3),
                                        (1.0, 4)])
-def test_cell_sizes(B, oracle, scene, cell, xsub, cuda):
+def test_cell_sizes(B, oracle, scene, cell, xsub, method, cuda):
     ps, ubis = scene
     u = ubis[:300]
     grid = B.GvecGrid(ps.gv, cell=cell, xsub=xsub)
-    c = B.score_grid(u, grid, [0.05, 0.1]).cpu().numpy()
+    if method == "bins" and not B.bins_fit(grid):
+        with pytest.raises(ValueError):
+            B.score_grid(u, grid, [0.05, 0.1], method=method)
+        method = None            # the default takes the lookup scorer for this grid
+    c = B.score_grid(u, grid, [0.05, 0.1], method=method).cpu().numpy()
     assert np.array_equal(c, oracle.score_many(u, ps.gv, [0.05, 0.1])), cell
 
 
-def test_ragged_and_empty(B, oracle, scene, cuda):
+@pytest.mark.parametrize("method", METHODS)
+def test_ragged_and_empty(B, oracle, scene, method, cuda):
     ps, ubis = scene
     for m, n in [(1, 1), (1, 1023), (3, 1025), (1025, 777), (257, 5000)]:
         g = ps.gv[:n]
         u = ubis[:m]
-        c = B.score_grid(u, B.GvecGrid(g), [0.05, 0.1]).cpu().numpy()
+        c = B.score_grid(u, B.GvecGrid(g), [0.05, 0.1], method=method).cpu().numpy()
         assert np.array_equal(c, oracle.score_many(u, g, [0.05, 0.1])), (m, n)
-    c = B.score_grid(np.eye(3)[None] * 4.05, B.GvecGrid(np.zeros((0, 3))), [0.1]).cpu().numpy()
+    c = B.score_grid(np.eye(3)[None] * 4.05, B.GvecGrid(np.zeros((0, 3))), [0.1],
+                     method=method).cpu().numpy()
     assert c.shape == (1, 1) and c[0, 0] == 0
-    c = B.score_grid(np.zeros((0, 3, 3)), B.GvecGrid(np.ones((10, 3))), [0.1])
+    c = B.score_grid(np.zeros((0, 3, 3)), B.GvecGrid(np.ones((10, 3))), [0.1], method=method)
     assert c.shape == (0, 1)
 
 
-def test_plain_scan_ubis_and_large_tols(B, oracle, scene, cuda):
+@pytest.mark.parametrize("method", METHODS)
+def test_plain_scan_ubis_and_large_tols(B, oracle, scene, method, cuda):
     ps, ubis = scene
     g = ps.gv[:20000]
     u = ubis[:40].copy()
@@ -99,7 +115,7 @@ def test_plain_scan_ubis_and_large_tols(B, oracle, scene, cuda):
     u[7] = 0.0                       # singular: every g has h = 0
     u[9] = np.diag([1e4, 1.0, 1e-4]) # condition number 1e8
     grid = B.GvecGrid(g)
-    c = B.score_grid(u, grid, [0.05, 0.1]).cpu().numpy()
+    c = B.score_grid(u, grid, [0.05, 0.1], method=method).cpu().numpy()
     assert np.array_equal(c, oracle.score_many(u, g, [0.05, 0.1]))
     assert grid.stats()["fallback_ubis"] == 4
     for tols in ([0.1, 0.47], [0.5, 0.9], [3.0]):
@@ -107,10 +123,11 @@ def test_plain_scan_ubis_and_large_tols(B, oracle, scene, cuda):
         assert np.array_equal(c, oracle.score_many(u, g, tols)), tols
 
 
-def test_matches_score_batch(B, scene, cuda):
+@pytest.mark.parametrize("method", METHODS)
+def test_matches_score_batch(B, scene, method, cuda):
     ps, ubis = scene
     tols = [0.01, 0.03, 0.07, 0.2]
-    a = B.score_grid(ubis, B.GvecGrid(ps.gv), tols).cpu().numpy()
+    a = B.score_grid(ubis, B.GvecGrid(ps.gv), tols, method=method).cpu().numpy()
     b = B.score_batch(ubis, B.GvecSet(ps.gv), tols).cpu().numpy()
     assert np.array_equal(a, b)
 
@@ -174,3 +191,55 @@ def test_random_sweep(B, oracle, cuda):
         tols = sorted(rng.uniform(0.001, 0.7, int(rng.integers(1, 5))).tolist())
         c = B.score_grid(ubis, B.GvecGrid(gv), tols).cpu().numpy()
         assert np.array_equal(c, oracle.score_many(ubis, gv, tols)), trial
+
+
+def test_bins_random_sweep(B, oracle, cuda):
+    """The binned join on random cells, orientations, g clouds (lattice g with
+    noise, g on rounding half-points) and tolerances below 0.4."""
+    rng = np.random.default_rng(78)
+    for trial in range(24):
+        n = int(rng.integers(1, 6000))
+        gv = rng.normal(size=(n, 3)) * rng.uniform(0.2, 2.0)
+        if trial % 3 == 1:
+            a = rng.uniform(2.0, 9.0)
+            hkl = rng.integers(-6, 7, size=(n, 3)).astype(float)
+            q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            gv = (hkl / a) @ q.T + rng.normal(scale=1e-3, size=(n, 3))
+        m = int(rng.integers(1, 300))
+        ubis = np.empty((m, 3, 3))
+        for i in range(m):
+            q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            ubis[i] = np.diag(rng.uniform(1.5, 12.0, 3)) @ q.T
+        if trial % 3 == 2:
+            gv[: n // 3] = np.linalg.solve(ubis[0], (rng.integers(-5, 5, (n // 3, 3)) + 0.5).T).T
+        tols = sorted(rng.uniform(0.001, 0.399, int(rng.integers(1, 5))).tolist())
+        grid = B.GvecGrid(gv, cell=float(rng.uniform(0.01, 0.2)) if trial % 2 else None)
+        if not B.bins_fit(grid):
+            grid = B.GvecGrid(gv)
+        c = B.score_grid(ubis, grid, tols, method="bins").cpu().numpy()
+        assert np.array_equal(c, oracle.score_many(ubis, gv, tols)), trial
+
+
+def test_bins_workspace_ranges(B, oracle, scene, cuda):
+    """A workspace holding only part of the boxes: the UBIs run in ranges,
+    with the same counts; too small for one UBI's boxes is an error."""
+    from imaged11_b200._lib import ID11BError
+    ps, ubis = scene
+    u = ubis[:200]
+    tols = [0.02, 0.05, 0.1]
+    grid = B.GvecGrid(ps.gv)
+    full = B.score_grid(u, grid, tols, method="bins").cpu().numpy()
+    assert np.array_equal(full, oracle.score_many(u, ps.gv, tols))
+    est = B.bins_box_estimate(u, grid, 0.1)
+    for frac in (0.5, 0.13):
+        ws = B.BinsWorkspace(len(u), grid, int(est * frac))
+        c = B.score_grid(u, grid, tols, method="bins", workspace=ws).cpu().numpy()
+        assert np.array_equal(c, full), frac
+    with pytest.raises(ID11BError):
+        B.score_grid(u, grid, tols, method="bins", workspace=B.BinsWorkspace(len(u), grid, 10))
+
+
+def test_bins_rejects_large_tolerances(B, scene, cuda):
+    ps, ubis = scene
+    with pytest.raises(Exception):
+        B.score_grid(ubis[:4], B.GvecGrid(ps.gv[:100]), [0.1, 0.4], method="bins")

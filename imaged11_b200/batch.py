@@ -188,7 +188,7 @@ class GvecGrid:
 
 BINS_TOL_LIMIT = 0.4   # the binned join takes tolerances below this
 BINS_MAX_BOXES = 1 << 29   # default workspace cap (4 GiB of boxes); more run in UBI ranges
-BINS_MAX_ROWS = 16384      # the binned join holds nx^2 rows of cells ...
+BINS_MAX_ROWS = 65536      # the binned join holds nx^2 rows of cells ...
 BINS_MAX_XCELLS = 8191     # ... and nx * xsub x cells per row
 
 

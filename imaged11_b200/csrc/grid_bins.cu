@@ -59,8 +59,9 @@ constexpr int kET = 32 * kEW;
 constexpr int kJT = 256;            // threads per join CTA (one row at a time)
 constexpr int kJW = kJT / 32;
 constexpr int kBMax = 4096;         // boxes of a row sorted in shared memory at a time
-constexpr int kGMax = 2048;         // g staged at a time (one tile)
-constexpr int kMaxRows = 16384;     // rows of cells (nx^2) the enumeration's counters hold
+constexpr int kGMax = 1536;         // g staged at a time (one tile)
+constexpr int kRowBlock = 16;       // rows of cells per block of the enumeration's streams
+constexpr int kMaxBlocks = 4096;    // blocks the enumeration's counters hold (nx^2 <= 65536)
 constexpr int kMaxNxx = 8191;       // x cells per row (13-bit field of a box record)
 constexpr int kMaxHalo = 1024;      // rows of cells around a row (the halo R: (2R+1)^2)
 constexpr int kMaxEnumCtas = 512;
@@ -68,7 +69,7 @@ constexpr double kTolLimit = 0.4;
 constexpr double kSGLimit = 16384.0;
 constexpr double kEps32 = 5.9604644775390625e-08;  // 2^-24
 constexpr int kHklOff = 256;        // hkl in 9-bit fields: -256 .. 255
-constexpr int kUbiBits = 24;        // UBI index (within a range of UBIs) in a box record
+constexpr int kUbiBits = 20;        // UBI index (within a range of UBIs) in a box record
 constexpr int kFallbackParts = 128; // warps per plainly scanned UBI
 constexpr int kBT = 128;            // threads per CTA of the exact scans
 constexpr int kBW = kBT / 32;
@@ -100,32 +101,41 @@ struct JoinParams {
     int64_t i0;                    // first UBI of the range (box records are relative to it)
 };
 
-// box record: UBI (24 bits, relative) | h + 256 (9) | k + 256 (9) | l + 256 (9) | x cell (13)
-__device__ __forceinline__ uint64_t pack_box(int64_t u, int h, int k, int l, int fx) {
-    return ((uint64_t)u << 40) | ((uint64_t)(h + kHklOff) << 31) |
-           ((uint64_t)(k + kHklOff) << 22) | ((uint64_t)(l + kHklOff) << 13) | (uint64_t)fx;
+// box record (64 bits): UBI (20 bits, relative to the range) | h + 256 (9) |
+// k + 256 (9) | l + 256 (9) | row within its block of 16 (4) | x cell (13)
+__device__ __forceinline__ uint64_t pack_box(int64_t u, int h, int k, int l, int rowlo, int fx) {
+    return ((uint64_t)u << 44) | ((uint64_t)(h + kHklOff) << 35) |
+           ((uint64_t)(k + kHklOff) << 26) | ((uint64_t)(l + kHklOff) << 17) |
+           ((uint64_t)rowlo << 13) | (uint64_t)fx;
 }
 __device__ __forceinline__ int box_fx(uint64_t r) { return (int)(r & 8191u); }
+__device__ __forceinline__ int box_rowlo(uint64_t r) { return (int)((r >> 13) & 15u); }
 
 struct BinLayout {
-    size_t info, packs, cnt_ubi, fallback, cta_rows, rowtot, rstart, tot, recs, bytes;
+    size_t info, packs, cnt_ubi, fallback, cta_blk, blktot, blkstart, rstart, tot, tmp, recs,
+        bytes;
 };
 
 // workspace: info | packs (m x 3 float4) | per-UBI box counts | fallback list |
-// per-CTA row counts / offsets | row totals | row starts | scan totals | boxes
+// per-CTA block counts / offsets | block totals | block starts | row starts |
+// scan totals | boxes by block | boxes by row
 inline BinLayout bin_layout(int64_t m, int64_t nrows, int64_t cap) {
     BinLayout L;
     const size_t mm = (size_t)(m > 0 ? m : 1);
+    const int64_t nblk = (nrows + kRowBlock - 1) / kRowBlock;
+    const size_t cc = (size_t)(cap > 0 ? cap : 1);
     size_t o = 0;
     L.info = o;     o = al256(o + sizeof(BinInfo));
     L.packs = o;    o = al256(o + 3 * sizeof(float4) * mm);
     L.cnt_ubi = o;  o = al256(o + sizeof(int) * mm);
     L.fallback = o; o = al256(o + sizeof(int) * mm);
-    L.cta_rows = o; o = al256(o + sizeof(int) * (size_t)kMaxEnumCtas * (size_t)nrows);
-    L.rowtot = o;   o = al256(o + sizeof(int) * (size_t)(nrows + 1));
+    L.cta_blk = o;  o = al256(o + sizeof(int) * (size_t)kMaxEnumCtas * (size_t)nblk);
+    L.blktot = o;   o = al256(o + sizeof(int) * (size_t)(nblk + 1));
+    L.blkstart = o; o = al256(o + sizeof(int) * (size_t)(nblk + 1));
     L.rstart = o;   o = al256(o + sizeof(int) * (size_t)(nrows + 1));
-    L.tot = o;      o = al256(o + sizeof(int) * (size_t)((nrows + 1 + kScanPer - 1) / kScanPer + 1));
-    L.recs = o;     o = al256(o + sizeof(uint64_t) * (size_t)(cap > 0 ? cap : 1));
+    L.tot = o;      o = al256(o + sizeof(int) * (size_t)((nblk + 1 + kScanPer - 1) / kScanPer + 1));
+    L.tmp = o;      o = al256(o + sizeof(uint64_t) * cc);
+    L.recs = o;     o = al256(o + sizeof(uint64_t) * cc);
     L.bytes = o;
     return L;
 }
@@ -188,28 +198,30 @@ __device__ __forceinline__ void make_plan32(const volatile WarpPlan* wp, const H
     *wmax = wm;
 }
 
-// mode 0 counts the boxes per row of cells (and, in the first pass, writes
-// the plans' FP32 packs, the largest widened half width and row sum, the
-// per-UBI box counts and the fallback list); mode 1 writes every box.  CTA c
-// takes UBIs i0 + [c * per, (c + 1) * per), its warps one UBI at a time in a
-// fixed order, and keeps one counter per row in shared memory: mode 0 stores
-// them in cta_rows[c][row]; mode 1 starts them at rstart[row] + cta_rows[c][row]
-// (the CTA's offset inside the row) and writes each box at its counter.  The
-// mode is a run-time argument of one kernel, so both passes run the same
-// machine code and put every box in the same row; each write is still bounded
-// by its row's range.
+// mode 0 counts the boxes per block of kRowBlock rows of cells (and, in the
+// first pass, writes the plans' FP32 packs, the largest widened half width and
+// row sum, the per-UBI box counts and the fallback list); mode 1 writes every
+// box.  CTA c takes UBIs i0 + [c * per, (c + 1) * per), its warps one UBI at
+// a time in a fixed order, and keeps one counter per block in shared memory:
+// mode 0 stores them in cta_blk[c][block]; mode 1 starts them at
+// blkstart[block] + cta_blk[c][block] (the CTA's offset inside the block) and
+// writes each box at its counter.  So every CTA writes one sequential stream
+// per block (few enough streams that L2 fills their lines before it evicts
+// them).  The mode is a run-time argument of one kernel, so both passes run
+// the same machine code and put every box in the same block; each write is
+// still bounded by the capacity of the box array.
 __global__ void __launch_bounds__(kET)
 k_enum(int mode, const double* __restrict__ ubis, int64_t i0, int64_t mc, int64_t per,
        const Header* __restrict__ Hp, const int* __restrict__ start, double tmax, int first,
-       int nrows, BinInfo* __restrict__ info, float4* __restrict__ packs,
-       int* __restrict__ cnt_ubi, int* __restrict__ fallback, int* __restrict__ cta_rows,
-       const int* __restrict__ rstart, uint64_t* __restrict__ recs) {
-    extern __shared__ int s_rows[];
+       int nblk, BinInfo* __restrict__ info, float4* __restrict__ packs,
+       int* __restrict__ cnt_ubi, int* __restrict__ fallback, int* __restrict__ cta_blk,
+       const int* __restrict__ blkstart, uint64_t* __restrict__ tmp, int64_t cap) {
+    __shared__ int s_blk[kMaxBlocks];
     __shared__ WarpPlan s_plan[kEW];
     __shared__ Plan32 s_p32[kEW];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int* my = cta_rows + (int64_t)blockIdx.x * nrows;
-    for (int r = threadIdx.x; r < nrows; r += kET) s_rows[r] = mode == 0 ? 0 : rstart[r] + my[r];
+    int* my = cta_blk + (int64_t)blockIdx.x * nblk;
+    for (int b = threadIdx.x; b < nblk; b += kET) s_blk[b] = mode == 0 ? 0 : blkstart[b] + my[b];
     __syncthreads();
     const Header H = *Hp;
     const int64_t nreg = start[H.ncells];
@@ -314,11 +326,11 @@ k_enum(int mode, const double* __restrict__ ubis, int64_t i0, int64_t mc, int64_
                         const int cy = min(max(__float2int_rd((c[1] - flo) * inv_cs), 0), H.nx - 1);
                         const int cz = min(max(__float2int_rd((c[2] - flo) * inv_cs), 0), H.nx - 1);
                         const int row = cz * H.nx + cy;
-                        const int slot = atomicAdd(s_rows + row, 1);
+                        const int slot = atomicAdd(s_blk + row / kRowBlock, 1);
                         if (mode == 0) {
                             nbox++;
-                        } else if (slot < rstart[row + 1]) {
-                            recs[slot] = pack_box(u, hj, kj, lj, cx);
+                        } else if (slot < cap) {
+                            tmp[slot] = pack_box(u, hj, kj, lj, row % kRowBlock, cx);
                         }
                     }
                 }
@@ -334,84 +346,128 @@ k_enum(int mode, const double* __restrict__ ubis, int64_t i0, int64_t mc, int64_
     }
     __syncthreads();
     if (mode == 0)
-        for (int r = threadIdx.x; r < nrows; r += kET) my[r] = s_rows[r];
+        for (int b = threadIdx.x; b < nblk; b += kET) my[b] = s_blk[b];
 }
 
-// Per row: the CTAs' counts turned into exclusive offsets inside the row (in
-// place), and the row's total.  One warp per row.
+// Per block: the CTAs' counts turned into exclusive offsets inside the block
+// (in place), and the block's total.  One warp per block.
 __global__ void __launch_bounds__(kGT)
-k_row_offsets(int* __restrict__ cta_rows, int nctas, int nrows, int* __restrict__ rowtot) {
+k_blk_offsets(int* __restrict__ cta_blk, int nctas, int nblk, int* __restrict__ blktot) {
     const int lane = threadIdx.x & 31;
-    for (int64_t r = ((int64_t)blockIdx.x * kGT + threadIdx.x) >> 5; r < nrows;
-         r += ((int64_t)gridDim.x * kGT) >> 5) {
+    for (int64_t b = ((int64_t)blockIdx.x * kGT + threadIdx.x) >> 5; b < nblk;
+         b += ((int64_t)gridDim.x * kGT) >> 5) {
         int run = 0;
         for (int c0 = 0; c0 < nctas; c0 += 32) {
             const int c = c0 + lane;
-            const int v = c < nctas ? cta_rows[(int64_t)c * nrows + r] : 0;
+            const int v = c < nctas ? cta_blk[(int64_t)c * nblk + b] : 0;
             int tot;
             const int ex = warp_excl_scan(v, lane, tot);
-            if (c < nctas) cta_rows[(int64_t)c * nrows + r] = run + ex;
+            if (c < nctas) cta_blk[(int64_t)c * nblk + b] = run + ex;
             run += tot;
         }
-        if (lane == 0) rowtot[r] = run;
+        if (lane == 0) blktot[b] = run;
     }
 }
 
-// ----------------------------------------------------------------- join ----
+// The boxes of each block split into its kRowBlock rows (any order within a
+// row): one CTA per block, each thread taking kRK boxes at a time (loads in
+// flight), counts and then cursors per (warp, row) in shared memory, so each
+// warp writes one sequential stream per row.  Both passes give each box to the
+// same thread.  Writes each row's start to rstart.
+constexpr int kRS = 512;
+constexpr int kRSW = kRS / 32;
+constexpr int kRK = 8;
+
+__global__ void __launch_bounds__(kRS)
+k_rowsplit(const uint64_t* __restrict__ tmp, const int* __restrict__ blkstart, int nblk,
+           int nrows, int* __restrict__ rstart, uint64_t* __restrict__ recs) {
+    __shared__ int s_wh[kRSW][kRowBlock];
+    const int w = threadIdx.x >> 5;
+    for (int b = blockIdx.x; b < nblk; b += gridDim.x) {
+        const int p0 = blkstart[b], p1 = blkstart[b + 1];
+        if (threadIdx.x < kRSW * kRowBlock) s_wh[threadIdx.x / kRowBlock][threadIdx.x % kRowBlock] = 0;
+        __syncthreads();
+        for (int i0 = p0; i0 < p1; i0 += kRS * kRK) {
+            uint64_t r[kRK];
+#pragma unroll
+            for (int k = 0; k < kRK; k++) {
+                const int i = i0 + k * kRS + threadIdx.x;
+                r[k] = i < p1 ? __ldg(tmp + i) : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < kRK; k++)
+                if (i0 + k * kRS + (int)threadIdx.x < p1) atomicAdd(&s_wh[w][box_rowlo(r[k])], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {  // per-warp cursors: rows in order, warps in order inside a row
+            int run = p0;
+            for (int v = 0; v < kRowBlock; v++) {
+                const int row = b * kRowBlock + v;
+                if (row < nrows) rstart[row] = run;
+                for (int q = 0; q < kRSW; q++) {
+                    const int c = s_wh[q][v];
+                    s_wh[q][v] = run;
+                    run += c;
+                }
+            }
+            if (b == nblk - 1) rstart[nrows] = run;
+        }
+        __syncthreads();
+        for (int i0 = p0; i0 < p1; i0 += kRS * kRK) {
+            uint64_t r[kRK];
+#pragma unroll
+            for (int k = 0; k < kRK; k++) {
+                const int i = i0 + k * kRS + threadIdx.x;
+                r[k] = i < p1 ? __ldg(tmp + i) : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < kRK; k++)
+                if (i0 + k * kRS + (int)threadIdx.x < p1)
+                    recs[atomicAdd(&s_wh[w][box_rowlo(r[k])], 1)] = r[k];
+        }
+        __syncthreads();
+    }
+}
+
 // A pair inside a band (or, with sums, any pair below hmax): the reference's
-// exact FP64 drlv2.  Returns the tolerances (bit j) for which it counts and
-// its drlv2.  Out of line: rare, and its registers would otherwise weigh on
-// the whole join.
-template <int NT>
-__device__ __noinline__ unsigned exact_pair(const double* __restrict__ ubis, int64_t ubi,
-                                            const double* __restrict__ gs, int pos, float hk0,
-                                            float hk1, float hk2, const double* t2,
-                                            double* s64) {
+// exact FP64 drlv2 and whether it belongs to the box's hkl, by value.  Out of
+// line: rare, and its registers would otherwise weigh on the whole join.
+struct Exact {
+    double s;   // drlv2
+    bool own;   // the rounded h is the box's hkl
+};
+
+__device__ __noinline__ Exact exact_pair(const double* __restrict__ ubis, int64_t ubi,
+                                         const double* __restrict__ gs, int pos, float hk0,
+                                         float hk1, float hk2) {
     double u[9], ih[3];
 #pragma unroll
     for (int e = 0; e < 9; e++) u[e] = __ldg(ubis + 9 * ubi + e);
-    const double s = drlv2_exact(u, __ldg(gs + 3 * (int64_t)pos), __ldg(gs + 3 * (int64_t)pos + 1),
-                                 __ldg(gs + 3 * (int64_t)pos + 2), ih);
-    *s64 = s;
-    if (!(ih[0] == (double)hk0 && ih[1] == (double)hk1 && ih[2] == (double)hk2)) return 0u;
-    unsigned m = 0u;
-#pragma unroll
-    for (int j = 0; j < NT; j++)
-        if (s < t2[j]) m |= 1u << j;
-    return m;
+    Exact r;
+    r.s = drlv2_exact(u, __ldg(gs + 3 * (int64_t)pos), __ldg(gs + 3 * (int64_t)pos + 1),
+                      __ldg(gs + 3 * (int64_t)pos + 2), ih);
+    r.own = ih[0] == (double)hk0 && ih[1] == (double)hk1 && ih[2] == (double)hk2;
+    return r;
 }
 
-// One screening value against the tolerances; rare pairs go exact.
+// A pair inside a band (or, with sums, any pair below hmax), evaluated
+// exactly: counted for the tolerances its FP64 drlv2 clears under its own hkl
+// (those it cleared in FP32 by more than the band were counted already).
 template <int NT, bool SUMS>
-__device__ __forceinline__ void count_pair(float s, const int* pos, const JoinParams& P,
-                                           const double* __restrict__ ubis, int64_t ubi,
-                                           const double* __restrict__ gs, const float* hkf,
-                                           int cnt[NT], double sum[NT], unsigned& ntest) {
-    bool exact = false;
-    if (SUMS) {
-        exact = s < P.hmax;
-    } else {
+__device__ __forceinline__ void rare_pair(float s, int pos, const JoinParams& P,
+                                          const double* __restrict__ ubis, int64_t ubi,
+                                          const double* __restrict__ gs, const float* hkf,
+                                          int cnt[NT], double sum[NT]) {
+    const Exact e = exact_pair(ubis, ubi, gs, pos, hkf[0], hkf[1], hkf[2]);
+    if (!e.own) return;
 #pragma unroll
-        for (int j = 0; j < NT; j++) {
-            const bool in = s < P.lo[j];
-            cnt[j] += in;
-            exact |= !in && s < P.hi[j];
-        }
-    }
-    if (exact) {
-        ntest++;
-        double s64;
-        const unsigned mk = exact_pair<NT>(ubis, ubi, gs, *pos, hkf[0], hkf[1], hkf[2], P.t2, &s64);
-#pragma unroll
-        for (int j = 0; j < NT; j++) {
-            if (SUMS) {
-                if (mk >> j & 1u) {
-                    cnt[j]++;
-                    sum[j] += s64;
-                }
-            } else if (!(s < P.lo[j]) && (mk >> j & 1u)) {
-                cnt[j]++;
-            }
+    for (int j = 0; j < NT; j++) {
+        if (!(e.s < P.t2[j])) continue;
+        if (SUMS) {
+            cnt[j]++;
+            sum[j] += e.s;
+        } else if (!(s < P.lo[j])) {
+            cnt[j]++;
         }
     }
 }
@@ -421,28 +477,19 @@ struct Staged {  // the tile of staged g, structure of arrays (pairs read as 64 
     const int* pos;
 };
 
-// The box of one lane against staged g [ga, gb): a single g first if ga is
-// odd, then pairs with packed f32x2 instructions (the same operations as
-// drlv2_f32 lane by lane, so every screening value is the scalar one), then a
-// single last g.
+// The box of one lane against staged g [ga, gb), two at a time with packed
+// f32x2 instructions (lane by lane the operations of drlv2_f32, so every
+// screening value is the scalar one).  The range is widened to even bounds
+// (an odd tile ends with a NaN g): testing g beyond a run's range is harmless,
+// every g of a tile being tested at most once per box.  Counting is free of
+// branches; one branch per pair of g catches the rare band cases.
 template <int NT, bool SUMS>
-__device__ __forceinline__ void test_range(const Staged& t, int ga, int gb, const float u[9],
-                                           const uint64_t uu[9], const uint64_t hh[3],
-                                           const float* hkf, const JoinParams& P,
-                                           const double* __restrict__ ubis, int64_t ubi,
-                                           const double* __restrict__ gs, int cnt[NT],
+__device__ __forceinline__ void test_range(const Staged& t, int ga, int gb, const uint64_t uu[9],
+                                           const uint64_t hh[3], const float* hkf,
+                                           const JoinParams& P, const double* __restrict__ ubis,
+                                           int64_t ubi, const double* __restrict__ gs, int cnt[NT],
                                            double sum[NT], unsigned& ntest) {
-    auto single = [&](int q) {
-        const float gx = t.x[q], gy = t.y[q], gz = t.z[q];
-        const float d0 = fmaf(u[2], gz, fmaf(u[1], gy, u[0] * gx)) - hkf[0];
-        const float d1 = fmaf(u[5], gz, fmaf(u[4], gy, u[3] * gx)) - hkf[1];
-        const float d2 = fmaf(u[8], gz, fmaf(u[7], gy, u[6] * gx)) - hkf[2];
-        count_pair<NT, SUMS>(fmaf(d2, d2, fmaf(d1, d1, d0 * d0)), t.pos + q, P, ubis, ubi, gs,
-                             hkf, cnt, sum, ntest);
-    };
-    int q = ga;
-    if (q < gb && (q & 1)) single(q++);
-    for (; q + 1 < gb; q += 2) {
+    for (int q = ga & ~1; q < gb; q += 2) {
         const uint64_t gx = *reinterpret_cast<const uint64_t*>(t.x + q);
         const uint64_t gy = *reinterpret_cast<const uint64_t*>(t.y + q);
         const uint64_t gz = *reinterpret_cast<const uint64_t*>(t.z + q);
@@ -452,10 +499,26 @@ __device__ __forceinline__ void test_range(const Staged& t, int ga, int gb, cons
         const uint64_t d0 = sub2(h0, hh[0]), d1 = sub2(h1, hh[1]), d2 = sub2(h2, hh[2]);
         float sa, sb;
         upk2(fma2(d2, d2, fma2(d1, d1, mul2(d0, d0))), sa, sb);
-        count_pair<NT, SUMS>(sa, t.pos + q, P, ubis, ubi, gs, hkf, cnt, sum, ntest);
-        count_pair<NT, SUMS>(sb, t.pos + q + 1, P, ubis, ubi, gs, hkf, cnt, sum, ntest);
+        bool ra, rb;
+        if (SUMS) {
+            ra = sa < P.hmax;
+            rb = sb < P.hmax;
+        } else {
+            ra = rb = false;
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                const bool ia = sa < P.lo[j], ib = sb < P.lo[j];
+                cnt[j] += (int)ia + (int)ib;
+                ra |= !ia && sa < P.hi[j];
+                rb |= !ib && sb < P.hi[j];
+            }
+        }
+        if (ra || rb) {
+            ntest += (unsigned)ra + (unsigned)rb;
+            if (ra) rare_pair<NT, SUMS>(sa, t.pos[q], P, ubis, ubi, gs, hkf, cnt, sum);
+            if (rb) rare_pair<NT, SUMS>(sb, t.pos[q + 1], P, ubis, ubi, gs, hkf, cnt, sum);
+        }
     }
-    if (q < gb) single(q);
 }
 
 // Exclusive scan of a[0 .. len) into b (block-wide; ends with a barrier).
@@ -480,7 +543,14 @@ __device__ __forceinline__ void block_scan(const int* a, int* b, int len, int* s
     __syncthreads();
 }
 
-// Persistent CTAs, each taking one row of cells at a time (a counter).
+// Persistent CTAs, each taking one row of cells at a time (a counter).  The
+// row's boxes are counted per x cell, the row is cut into windows of x cells
+// holding at most kBMax boxes (a cell with more is taken alone, in pieces of
+// kBMax boxes in storage order), and each window's boxes are placed in shared
+// memory sorted by x cell.  The g-vectors of the window's region are staged in
+// tiles of at most kGMax, each sorted by x cell, and every run of 32 sorted
+// boxes (one warp) is tested against the staged g in the x cells its boxes
+// can reach.
 template <int NT, bool SUMS>
 __global__ void __launch_bounds__(kJT, kJoinMinBlocks)
 k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nrows,
@@ -495,11 +565,13 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
     float* s_gz = s_gy + kGMax;
     int* s_gp = reinterpret_cast<int*>(s_gz + kGMax);
     const int nh1 = max(P.nxx, nhalo) + 1;
-    int* s_h = s_gp + kGMax;                                    // counts / cursors (nh1)
-    int* s_s = s_h + nh1;                                       // exclusive starts (nh1)
-    int* s_rp = s_s + nh1;                                      // halo rows: candidate prefix
-    int* s_rs = s_rp + (nhalo + 1);                             // halo rows: first g
-    __shared__ int s_row, s_w[kJW];
+    int* s_bs = s_gp + kGMax;        // boxes of the row before each x cell (nxx + 1)
+    int* s_bc = s_bs + nh1;          // box counts, then cursors
+    int* s_gh = s_bc + nh1;          // halo row lengths; g counts / cursors
+    int* s_gs = s_gh + nh1;          // staged g before each x cell of the tile
+    int* s_rp = s_gs + nh1;          // halo rows: candidate prefix (nhalo + 1)
+    int* s_rs = s_rp + (nhalo + 1);  // halo rows: first g
+    __shared__ int s_row, s_w[kJW], s_base;
     const Staged T{s_gx, s_gy, s_gz, s_gp};
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned ntest = 0;
@@ -517,56 +589,96 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
         const int ry0 = max(iy - P.R, 0), rz0 = max(iz - P.R, 0);
         const int ny = min(iy + P.R, P.nx - 1) - ry0 + 1;
         const int nhr = ny * (min(iz + P.R, P.nx - 1) - rz0 + 1);
-        for (int p0 = b0; p0 < b1; p0 += kBMax) {
-            const int nb = min(kBMax, b1 - p0);
-            // the part's boxes sorted by x cell
-            for (int x = threadIdx.x; x <= P.nxx; x += kJT) s_h[x] = 0;
-            __syncthreads();
-            for (int i = threadIdx.x; i < nb; i += kJT) atomicAdd(s_h + box_fx(recs[p0 + i]), 1);
-            __syncthreads();
-            block_scan(s_h, s_s, P.nxx + 1, s_w);
-            for (int x = threadIdx.x; x <= P.nxx; x += kJT) s_h[x] = 0;
-            __syncthreads();
-            for (int i = threadIdx.x; i < nb; i += kJT) {
-                const uint64_t rec = recs[p0 + i];
-                const int fx = box_fx(rec);
-                s_box[s_s[fx] + atomicAdd(s_h + fx, 1)] = rec;
+        // the row's boxes per x cell
+        for (int x = threadIdx.x; x <= P.nxx; x += kJT) s_bc[x] = 0;
+        __syncthreads();
+        for (int i = b0 + threadIdx.x; i < b1; i += kJT) atomicAdd(s_bc + box_fx(recs[i]), 1);
+        __syncthreads();
+        block_scan(s_bc, s_bs, P.nxx + 1, s_w);
+        int wa = 0, piece = 0;
+        while (wa < P.nxx) {  // uniform over the CTA
+            int lo = wa, hi = P.nxx;  // the largest wb with s_bs[wb] - s_bs[wa] <= kBMax
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_bs[mid] - s_bs[wa] <= kBMax) lo = mid; else hi = mid - 1;
+            }
+            const bool big = lo == wa;  // cell wa alone holds more than kBMax boxes
+            const int wb = big ? wa + 1 : lo;
+            const int skip = big ? piece * kBMax : 0;
+            const int ncell = s_bs[wb] - s_bs[wa];
+            const int nb = big ? min(kBMax, ncell - skip) : ncell;
+            const int cur_wa = wa;
+            if (big && skip + nb < ncell) {
+                piece++;
+            } else {
+                piece = 0;
+                wa = wb;
+            }
+            if (nb == 0) continue;
+            // the window's boxes in shared memory, sorted by x cell
+            if (!big) {
+                for (int x = cur_wa + threadIdx.x; x < wb; x += kJT) s_bc[x] = 0;
+                __syncthreads();
+                for (int i = b0 + threadIdx.x; i < b1; i += kJT) {
+                    const uint64_t rec = recs[i];
+                    const int fx = box_fx(rec);
+                    if (fx >= cur_wa && fx < wb)
+                        s_box[s_bs[fx] - s_bs[cur_wa] + atomicAdd(s_bc + fx, 1)] = rec;
+                }
+            } else {  // boxes skip .. skip + nb - 1 of cell cur_wa, in storage order
+                if (threadIdx.x == 0) s_base = 0;
+                __syncthreads();
+                for (int i0 = b0; i0 < b1; i0 += kJT) {
+                    const int i = i0 + threadIdx.x;
+                    uint64_t rec = 0;
+                    const bool mine = i < b1 && box_fx(rec = recs[i]) == cur_wa;
+                    const unsigned bal = __ballot_sync(0xffffffffu, mine);
+                    if (lane == 0) s_w[w] = __popc(bal);
+                    __syncthreads();
+                    int rank = s_base + __popc(bal & ((1u << lane) - 1u));
+                    for (int k = 0; k < w; k++) rank += s_w[k];
+                    if (mine && rank >= skip && rank < skip + nb) s_box[rank - skip] = rec;
+                    __syncthreads();
+                    if (threadIdx.x == 0)
+                        for (int k = 0; k < kJW; k++) s_base += s_w[k];
+                    __syncthreads();
+                }
             }
             __syncthreads();
-            // x cells the part's boxes can reach, and the halo rows' g in them
-            const int fxa = max(box_fx(s_box[0]) - P.Rx, 0);
-            const int fxb = min(box_fx(s_box[nb - 1]) + P.Rx, P.nxx - 1);
-            const int gw = fxb - fxa + 1;
+            // x cells the window's boxes can reach, and the halo rows' g in them
+            const int gxa = max(box_fx(s_box[0]) - P.Rx, 0);
+            const int gxb = min(box_fx(s_box[nb - 1]) + P.Rx, P.nxx - 1);
+            const int gw = gxb - gxa + 1;
             for (int j = threadIdx.x; j <= nhr; j += kJT) {
                 int len = 0;
                 if (j < nhr) {
                     const int zq = j / ny;
                     const int64_t base = ((int64_t)(rz0 + zq) * P.nx + (ry0 + j - zq * ny)) * P.nxx;
-                    const int st = start[base + fxa];
+                    const int st = start[base + gxa];
                     s_rs[j] = st;
-                    len = start[base + fxb + 1] - st;
+                    len = start[base + gxb + 1] - st;
                 }
-                s_h[j] = len;
+                s_gh[j] = len;
             }
             __syncthreads();
-            block_scan(s_h, s_rp, nhr + 1, s_w);
+            block_scan(s_gh, s_rp, nhr + 1, s_w);
             const int ncand = s_rp[nhr];
+            // candidate q: its g (w: its x cell) and position; true when inside
+            // the row's y/z region
+            auto candidate = [&](int q, float4& v, int& pos) {
+                int a = 0, c = nhr - 1;  // the last halo row with s_rp <= q
+                while (a < c) {
+                    const int mid = (a + c + 1) >> 1;
+                    if (s_rp[mid] <= q) a = mid; else c = mid - 1;
+                }
+                pos = s_rs[a] + (q - s_rp[a]);
+                v = __ldg(g4 + pos);
+                return v.y >= ylo && v.y <= yhi && v.z >= zlo && v.z <= zhi;
+            };
             // tiles of at most kGMax staged g, each sorted by x cell
             for (int c0 = 0; c0 < ncand;) {
-                for (int x = threadIdx.x; x <= gw; x += kJT) s_h[x] = 0;
+                for (int x = threadIdx.x; x <= gw; x += kJT) s_gh[x] = 0;
                 __syncthreads();
-                // candidate q: its g (w: its x cell) and position; true when
-                // inside the row's y/z region
-                auto candidate = [&](int q, float4& v, int& pos) {
-                    int lo = 0, hi = nhr - 1;              // last halo row with s_rp <= q
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (s_rp[mid] <= q) lo = mid; else hi = mid - 1;
-                    }
-                    pos = s_rs[lo] + (q - s_rp[lo]);
-                    v = __ldg(g4 + pos);
-                    return v.y >= ylo && v.y <= yhi && v.z >= zlo && v.z <= zhi;
-                };
                 int cend = c0, tot = 0;
                 while (cend < ncand && tot <= kGMax - kJT) {
                     const int q = cend + threadIdx.x;
@@ -575,38 +687,45 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
                         float4 v;
                         int pos;
                         in = candidate(q, v, pos);
-                        if (in) atomicAdd(s_h + (__float_as_int(v.w) - fxa), 1);
+                        if (in) atomicAdd(s_gh + (__float_as_int(v.w) - gxa), 1);
                     }
                     tot += __syncthreads_count(in);
                     cend = min(cend + kJT, ncand);
                 }
-                block_scan(s_h, s_s, gw + 1, s_w);
-                for (int x = threadIdx.x; x <= gw; x += kJT) s_h[x] = 0;
+                block_scan(s_gh, s_gs, gw + 1, s_w);
+                for (int x = threadIdx.x; x <= gw; x += kJT) s_gh[x] = 0;
                 __syncthreads();
                 for (int q = c0 + threadIdx.x; q < cend; q += kJT) {
                     float4 v;
                     int pos;
                     if (candidate(q, v, pos)) {
-                        const int cx = __float_as_int(v.w) - fxa;
-                        const int slot = s_s[cx] + atomicAdd(s_h + cx, 1);
+                        const int cx = __float_as_int(v.w) - gxa;
+                        const int slot = s_gs[cx] + atomicAdd(s_gh + cx, 1);
                         s_gx[slot] = v.x;
                         s_gy[slot] = v.y;
                         s_gz[slot] = v.z;
                         s_gp[slot] = pos;
                     }
                 }
+                if (threadIdx.x == 0 && (s_gs[gw] & 1)) {  // pad an odd tile with a NaN g
+                    const float nan = __int_as_float(0x7fc00000);
+                    s_gx[s_gs[gw]] = nan;
+                    s_gy[s_gs[gw]] = nan;
+                    s_gz[s_gs[gw]] = nan;
+                    s_gp[s_gs[gw]] = 0;
+                }
                 __syncthreads();
                 // runs of 32 sorted boxes, one warp each
                 for (int k0 = 32 * w; k0 < nb; k0 += 32 * kJW) {
                     const int nrun = min(32, nb - k0);
-                    const int ga = s_s[max(box_fx(s_box[k0]) - P.Rx, fxa) - fxa];
-                    const int gb = s_s[min(box_fx(s_box[k0 + nrun - 1]) + P.Rx, fxb) - fxa + 1];
+                    const int ga = s_gs[max(box_fx(s_box[k0]) - P.Rx, gxa) - gxa];
+                    const int gb = s_gs[min(box_fx(s_box[k0 + nrun - 1]) + P.Rx, gxb) - gxa + 1];
                     if (lane < nrun && ga < gb) {
                         const uint64_t rec = s_box[k0 + lane];
-                        const int64_t ubi = P.i0 + (int64_t)(rec >> 40);
-                        const float hkf[3] = {(float)((int)((rec >> 31) & 511) - kHklOff),
-                                              (float)((int)((rec >> 22) & 511) - kHklOff),
-                                              (float)((int)((rec >> 13) & 511) - kHklOff)};
+                        const int64_t ubi = P.i0 + (int64_t)(rec >> 44);
+                        const float hkf[3] = {(float)((int)((rec >> 35) & 511) - kHklOff),
+                                              (float)((int)((rec >> 26) & 511) - kHklOff),
+                                              (float)((int)((rec >> 17) & 511) - kHklOff)};
                         const float4 p0 = __ldg(packs + 3 * ubi);
                         const float4 p1 = __ldg(packs + 3 * ubi + 1);
                         const float4 p2 = __ldg(packs + 3 * ubi + 2);
@@ -623,7 +742,7 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
                             cnt[j] = 0;
                             sum[j] = 0.;
                         }
-                        test_range<NT, SUMS>(T, ga, gb, u, uu, hh, hkf, P, ubis, ubi, gs, cnt, sum,
+                        test_range<NT, SUMS>(T, ga, gb, uu, hh, hkf, P, ubis, ubi, gs, cnt, sum,
                                              ntest);
 #pragma unroll
                         for (int j = 0; j < NT; j++) {
@@ -831,11 +950,12 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     if (m > INT32_MAX - 1) return ID11B_ERR_SIZE;
     const int nrows = nx * nx;
     const int nxx = nx * xsub;
-    if (nrows > kMaxRows || nxx > kMaxNxx) return ID11B_ERR_SIZE;  // use id11b_dev_score_grid
+    const int nblk = (nrows + kRowBlock - 1) / kRowBlock;
+    if (nblk > kMaxBlocks || nxx > kMaxNxx) return ID11B_ERR_SIZE;  // use id11b_dev_score_grid
     // the largest box capacity the workspace holds
     const BinLayout L0 = bin_layout(m, nrows, 0);
     if (ws_bytes < (int64_t)L0.bytes) return ID11B_ERR_SIZE;
-    int64_t cap = (ws_bytes - (int64_t)L0.bytes) / (int64_t)sizeof(uint64_t);
+    int64_t cap = (ws_bytes - (int64_t)L0.bytes) / (int64_t)(2 * sizeof(uint64_t));
     while (cap > 0 && (int64_t)bin_layout(m, nrows, cap).bytes > ws_bytes) cap -= 1 + cap / 1024;
     if (cap > INT32_MAX - 1) cap = INT32_MAX - 1;
     const BinLayout B = bin_layout(m, nrows, cap);
@@ -851,10 +971,12 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     float4* packs = (float4*)(w + B.packs);
     int* cnt_ubi = (int*)(w + B.cnt_ubi);
     int* fallback = (int*)(w + B.fallback);
-    int* cta_rows = (int*)(w + B.cta_rows);
-    int* rowtot = (int*)(w + B.rowtot);
+    int* cta_blk = (int*)(w + B.cta_blk);
+    int* blktot = (int*)(w + B.blktot);
+    int* blkstart = (int*)(w + B.blkstart);
     int* rstart = (int*)(w + B.rstart);
     int* tot = (int*)(w + B.tot);
+    uint64_t* tmp = (uint64_t*)(w + B.tmp);
     uint64_t* recs = (uint64_t*)(w + B.recs);
     ID11B_CHECK(cudaMemsetAsync(&H->nfallback, 0, 2 * sizeof(unsigned long long), st));
     if (m == 0) return ID11B_OK;
@@ -862,17 +984,14 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     if (sums) ID11B_CHECK(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)(m * ntol), st));
     ID11B_CHECK(cudaMemsetAsync(info, 0, sizeof(BinInfo), st));
     // the enumeration's CTAs (same count and UBI ranges in both passes)
-    const size_t esmem = sizeof(int) * (size_t)nrows;
     static thread_local int enum_per_sm = 0;
-    if (!enum_per_sm) enum_per_sm = ctas_per_sm(k_enum, kET, 64 * 1024);
-    ID11B_CHECK(cudaFuncSetAttribute(k_enum, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)esmem));
+    if (!enum_per_sm) enum_per_sm = ctas_per_sm(k_enum, kET, 0);
     const int nctas = (int)std::min<int64_t>(kMaxEnumCtas, (int64_t)num_sms() * enum_per_sm);
     auto enumerate = [&](int mode, int64_t i0, int64_t mc, int first) {
         const int64_t per = (mc + nctas - 1) / nctas;
         const int grid = (int)std::min<int64_t>(nctas, (mc + per - 1) / per);
-        k_enum<<<grid, kET, esmem, st>>>(mode, ubis, i0, mc, per, H, start, tmax, first, nrows,
-                                         info, packs, cnt_ubi, fallback, cta_rows, rstart, recs);
+        k_enum<<<grid, kET, 0, st>>>(mode, ubis, i0, mc, per, H, start, tmax, first, nblk, info,
+                                     packs, cnt_ubi, fallback, cta_blk, blkstart, tmp, cap);
         return grid;
     };
     int egrid = enumerate(0, 0, m, 1);
@@ -940,7 +1059,7 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     const int nhalo = (2 * P.R + 1) * (2 * P.R + 1);
     if (bi.total > 0 && nhalo > kMaxHalo) return ID11B_ERR_SIZE;  // cells far smaller than W
     const size_t jsmem = sizeof(uint64_t) * kBMax + 4 * sizeof(float) * kGMax +
-                         2 * sizeof(int) * (size_t)(std::max(nxx, nhalo) + 1) +
+                         4 * sizeof(int) * (size_t)(std::max(nxx, nhalo) + 1) +
                          2 * sizeof(int) * (size_t)(nhalo + 1);
     const int jgrid = num_sms() * ID11B_BINS_DISPATCH(join_ctas, jsmem);
     for (size_t c = 0; c + 1 < cuts.size() && bi.total > 0; c++) {
@@ -949,13 +1068,16 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
             egrid = enumerate(0, i0, mc, 0);
             ID11B_CHECK_LAUNCH();
         }
-        k_row_offsets<<<grid_for((int64_t)nrows * 32, kGT), kGT, 0, st>>>(cta_rows, egrid, nrows,
-                                                                         rowtot);
+        k_blk_offsets<<<grid_for((int64_t)nblk * 32, kGT), kGT, 0, st>>>(cta_blk, egrid, nblk,
+                                                                        blktot);
         ID11B_CHECK_LAUNCH();
-        ID11B_CHECK(cudaMemsetAsync(rowtot + nrows, 0, sizeof(int), st));
-        int rc = scan(rowtot, nrows + 1, rstart, tot, st);
+        ID11B_CHECK(cudaMemsetAsync(blktot + nblk, 0, sizeof(int), st));
+        int rc = scan(blktot, nblk + 1, blkstart, tot, st);
         if (rc) return rc;
         enumerate(1, i0, mc, 0);
+        ID11B_CHECK_LAUNCH();
+        k_rowsplit<<<(unsigned)std::min(nblk, num_sms() * 4), kRS, 0, st>>>(tmp, blkstart, nblk,
+                                                                           nrows, rstart, recs);
         ID11B_CHECK_LAUNCH();
         ID11B_CHECK(cudaMemsetAsync(&info->next_row, 0, sizeof(int), st));
         P.i0 = i0;

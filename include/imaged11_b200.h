@@ -279,8 +279,9 @@ int id11b_grid_stats(const void *gridbuf, int64_t *nregular, int64_t *nspecial,
  * staged in shared memory, with the FP32 screening arithmetic; pairs inside
  * the proven error band are re-evaluated with the reference's FP64
  * arithmetic.  Tolerances must lie in [0, 0.4) (else ID11B_ERR_ARG: use
- * id11b_dev_score_grid).  The workspace (256-byte aligned) holds per-UBI,
- * per-cell and per-row tables plus 8.5 bytes per box:
+ * id11b_dev_score_grid; also for grids beyond 65,536 rows of cells or 8,191
+ * x cells per row, ID11B_ERR_SIZE).  The workspace (256-byte aligned) holds
+ * per-UBI and per-row tables plus 16 bytes per box:
  * id11b_grid_bins_workspace_bytes(m, nx, xsub, boxes) for a box capacity;
  * with fewer bytes than the call needs, the UBIs are processed in ranges that
  * fit (ID11B_ERR_SIZE when one UBI's boxes alone do not fit).  The call reads

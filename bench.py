@@ -4,12 +4,19 @@ Workload (default): 1.1M g-vectors simulated from 2,000 FCC Al grains
 (a = 4.05 A, |g| <= 1.5 A^-1, wavelength 0.2846 A, 150 mm, 2048^2 x 75 um
 detector, sigma 0.5 px / 0.05 deg centroid noise, 10% uniform noise peaks)
 scored against 20,000 trial UBIs (10% true orientations perturbed by 0.5 deg,
-90% uniformly random orientations of the same cell) at tol = 0.02, 0.05, 0.1
-in one launch sequence, counts identical to the reference's score().
+90% uniformly random orientations of the same cell) at tol = 0.02, 0.05, 0.1,
+counts identical to the reference's score().
 
 Metric: assigned peak x grain pairs per second = M * N * T / step time.
-One step = FP32 copy of the g-vectors + batched score (UBI packing, screening
-kernel, exact-FP64 list kernel), inputs resident in HBM.
+One step = the reciprocal-space cell index rebuilt from the g-vectors + exact
+batched scoring through it (binned join: FP32 screening of every (UBI, hkl)
+box against the g near it, proven FP64 recheck band), inputs resident in HBM.
+Beside it in the same run: the plain FP64 kernel (every pair, reference
+arithmetic) on the same 20,000 UBIs, the brute-force FP32 screening kernel,
+the per-box lookup scorer, the reference's own C on the host cores, and the
+other configurations (uneven refinement, adjoint, translations, the
+full-scale scan, the small drop-in sequence), each checked against the
+reference.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -30,8 +37,13 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 TOLS = [0.02, 0.05, 0.1]
-# DRAM bytes of one screening-kernel launch on this workload's g-vectors (ncu capture)
-K_BATCH_DRAM_BYTES = 19.8e6
+# DRAM bytes (read + write) of one binned-join launch on this workload, from an ncu
+# capture of the same command (profiles/): the traffic is the box records
+K_JOIN_DRAM_BYTES = 401.2e6
+K_JOIN_TRAFFIC_NOTE = ("dram__bytes_read.sum + dram__bytes_write.sum of one k_join<3> launch "
+                       "(20,000 UBIs, cell factor 0.8, x cut 8x; ncu capture named in "
+                       "profiles/k_join_binned_20000ubi_1.1Mg.md): mostly the box records, "
+                       "read once; the staged g come from L2")
 N_GRAINS = 2000
 GMAX = 1.5
 N_UBI = 20000
@@ -85,12 +97,11 @@ def grid_measure(torch, dev, ps, ubis, steps=5, flush=None, check_counts=None, c
     grid = batch.GvecGrid(gv_d, cell=cell, xsub=xsub)
     torch.cuda.synchronize()
     build_ms = (time.perf_counter() - t0) * 1e3
-    ws = torch.empty(batch.lib.id11b_grid_score_workspace_bytes(m, T), dtype=torch.uint8,
-                     device=dev)
+    ws = batch.BinsWorkspace(m, grid, batch.bins_box_estimate(ubis_d, grid, max(TOLS)))
     counts = torch.empty((m, T), dtype=torch.int32, device=dev)
 
     def run():
-        batch.score_grid(ubis_d, grid, TOLS, workspace=ws, out=counts)
+        batch.score_grid(ubis_d, grid, TOLS, workspace=ws, out=counts, method="bins")
     for _ in range(3):
         run()
     same = None
@@ -392,15 +403,20 @@ def adjoint_measure(torch, dev, steps=5, refine=True):
     return out
 
 
-def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5):
+def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
     """Full-scale scan: 20,000 grains (70% hcp Ti, 30% bcc beta-Ti, |g| <= 1.27,
     15% noise peaks, cfg3 geometry), end to end on the device:
-    compute_xlylzl + compute_gv -> cell index + scoring of n_ubi trial UBIs ->
-    batched score_and_assign of every peak to the 20,000 grains (their UBIs
-    0.2 deg / 0.2% off truth) -> peaks grouped by label -> `rounds` rounds of
-    per-grain refinement -> hkl of the assigned peaks from the refined UBIs ->
-    one residual gradient over 12 geometry parameters + every UBI.  The FP32
-    screening kernel on the same trial UBIs is timed beside it."""
+    compute_xlylzl + compute_gv -> cell index + scoring of n_ubi trial UBIs
+    (binned join) -> batched score_and_assign of every peak to the 20,000
+    grains (their UBIs 0.2 deg / 0.2% off truth) -> peaks grouped by label ->
+    `rounds` rounds of per-grain refinement -> hkl of the assigned peaks from
+    the refined UBIs -> one geometry step (one L-BFGS iteration on the 12
+    geometry parameters, every grain's UBI re-solved, driven by the adjoint).
+    Each stage's output is checked against the reference's own C on a sample
+    (cpu=True): compute_gv on 1M peaks, score() of 256 trials over all peaks,
+    the sequential score_and_assign of all 20,000 grains on 100k peaks, and 5
+    score_and_refine rounds of 64 grains on the same grouped peaks.  The FP32
+    screening kernel on the same trials is timed beside it."""
     from imaged11_b200 import adjoint, batch, synth
     from imaged11_b200 import cImageD11 as cim
     from imaged11_b200._lib import lib, check
@@ -420,29 +436,32 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5):
     om_d = torch.tensor(ps.omega, device=dev)
     xyz = torch.empty((n, 3), dtype=torch.float64, device=dev)
     gv = torch.empty((n, 3), dtype=torch.float64, device=dev)
-    gs = batch.GvecSet(torch.zeros((n, 3), dtype=torch.float64, device=dev))
+    g4 = torch.empty((n, 4), dtype=torch.float32, device=dev)
     ub_d = torch.tensor(trials, device=dev)
     u_ref = synth.perturb_ubis(ps.ubis, 0.2, 0.002, rng)
     u_ref_d = torch.tensor(u_ref, device=dev)
     stream = torch.cuda.current_stream().cuda_stream
     t_arr = np.array([truth["t_x"], truth["t_y"], truth["t_z"]])
-    gws = torch.empty(lib.id11b_grid_score_workspace_bytes(len(trials), 1), dtype=torch.uint8,
-                      device=dev)
     cbuf = torch.empty((len(trials), 1), dtype=torch.int32, device=dev)
     d2 = torch.empty(n, dtype=torch.float64, device=dev)
     lab = torch.empty(n, dtype=torch.int32, device=dev)
     out = {}
+    state = {}
 
-    def run(ev):
+    def run(ev, shape=None):
         ev[0].record()
         cim.compute_xlylzl(s_d, f_d, p, r.ravel(), dist, xyz)
         check(lib.id11b_dev_compute_gv(xyz.data_ptr(), om_d.data_ptr(), truth["omegasign"],
                                        truth["wavelength"], truth["wedge"], truth["chi"],
-                                       t_arr.ctypes.data, gv.data_ptr(), gs.g4.data_ptr(), n,
+                                       t_arr.ctypes.data, gv.data_ptr(), g4.data_ptr(), n,
                                        stream), "compute_gv")
         ev[1].record()
-        grid = batch.GvecGrid(gv)
-        batch.score_grid(ub_d, grid, [tol], workspace=gws, out=cbuf)
+        grid = batch.GvecGrid(gv) if shape is None else \
+            batch.GvecGrid(gv, cell=state["cs"], xsub=state["xsub"])
+        if "ws" not in state or (state["ws"].nx, state["ws"].xsub) != (grid.nx, grid.xsub):
+            state["boxes"] = batch.bins_box_estimate(ub_d, grid, tol)
+            state["ws"] = batch.BinsWorkspace(len(trials), grid, state["boxes"])
+        batch.score_grid(ub_d, grid, [tol], workspace=state["ws"], out=cbuf)
         ev[2].record()
         d2.fill_(2.0)
         lab.fill_(-1)
@@ -460,28 +479,33 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5):
         hkl = torch.round(torch.einsum("nij,nj->ni", ub_pk, grains.gv))
         peaks = adjoint.PeakTable(s_d.index_select(0, order), f_d.index_select(0, order),
                                   om_d.index_select(0, order), hkl, off, truth)
-        pt = adjoint.params_tensor(truth).requires_grad_(True)
-        ut = grains.ubis.view(-1, 3, 3).clone().requires_grad_(True)
-        adjoint.loss(pt, ut, peaks).backward()
+        p0 = adjoint.params_tensor(truth)
+        p1, _, hist = adjoint.refine_geometry(peaks, p0, max_iter=1)
         ev[5].record()
         ev[5].synchronize()
         out.update(assigned=int(n - first), refined_peaks=grains.peaks,
-                   npk_median=int(grains.npk.median().item()))
+                   npk_median=int(grains.npk.median().item()),
+                   geometry_step={"loss_before": hist[0], "loss_after": min(hist),
+                                  "evaluations": len(hist),
+                                  "step_applied": bool(min(hist) <= hist[0])})
+        state.update(grid=grid, order=order, off=off, grains=grains)
 
     run([torch.cuda.Event(enable_timing=True) for _ in range(6)])   # warm-up (module loads)
     # index shape for this peak set from the autotuner, on a tenth of the trials
     # (untimed setup; the counts do not depend on it)
     from imaged11_b200 import tune
-    shape, _ = tune.tune_grid(ub_d[::10], gv, [tol], cell_factors=(1.0, 1.25, 1.6),
-                              xsubs=(1, 2, 4), reps=1)
+    base = batch.GvecGrid(gv, xsub=1)
+    shape, _ = tune.tune_grid(ub_d[::10], gv, [tol], cell_factors=(0.8, 1.0, 1.25),
+                              xsubs=(2, 4, 8), reps=1)
+    state.update(cs=base.cs * shape[0], xsub=shape[1])
+    del base
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
-    run(ev)
+    run(ev, shape)
     names = ["compute_xlylzl+compute_gv", "cell_index+score_grid", "score_and_assign",
-             "group+refine_csr", "adjoint_gradient"]
+             "group+refine_csr", "adjoint_geometry_step"]
     stages = {nm: ev[i].elapsed_time(ev[i + 1]) for i, nm in enumerate(names)}
     # the FP32 screening kernel on the same trial UBIs, for comparison
-    gs.gv = gv
-    gs.prepare()
+    gs = batch.GvecSet(gv)
     ws = batch.BatchWorkspace(len(trials), n, refine=False)
     c32 = batch.score_batch(ub_d, gs, [tol], workspace=ws)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -489,18 +513,59 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5):
     c32 = batch.score_batch(ub_d, gs, [tol], workspace=ws)
     e1.record()
     e1.synchronize()
-    pairs = len(trials) * n + ng * n + rounds * out["refined_peaks"] + out["refined_peaks"]
+    pairs = (len(trials) * n + ng * n + rounds * out["refined_peaks"] +
+             out["geometry_step"]["evaluations"] * out["refined_peaks"])
     device_ms = sum(stages.values())
-    return {"grains": ng, "peaks": n, "trial_ubis": int(len(trials)), "tol": tol,
-            "stage_ms": stages, "pairs": pairs, "device_ms": device_ms,
-            "value": pairs / (device_ms * 1e-3), "unit": "pairs/s",
-            "assigned_peaks": out["assigned"], "peaks_per_grain_median": out["npk_median"],
-            "index_shape": {"cell_factor": shape[0], "xsub": shape[1]},
-            "score_batch_fp32_ms": e0.elapsed_time(e1),
-            "score_grid_counts_equal_fp32": bool(torch.equal(c32, cbuf)),
-            "trial_counts_median_max": [int(cbuf[:, 0].median().item()),
-                                        int(cbuf[:, 0].max().item())],
-            "note": "wall between events: host glue (grouping, GrainSet, PeakTable) included"}
+    res = {"grains": ng, "peaks": n, "trial_ubis": int(len(trials)), "tol": tol,
+           "stage_ms": stages, "pairs": pairs, "device_ms": device_ms,
+           "value": pairs / (device_ms * 1e-3), "unit": "pairs/s",
+           "assigned_peaks": out["assigned"], "peaks_per_grain_median": out["npk_median"],
+           "geometry_step": out["geometry_step"],
+           "index_shape": {"cell_factor": shape[0], "xsub": shape[1]},
+           "score_batch_fp32_ms": e0.elapsed_time(e1),
+           "score_grid_counts_equal_fp32": bool(torch.equal(c32, cbuf)),
+           "trial_counts_median_max": [int(cbuf[:, 0].median().item()),
+                                       int(cbuf[:, 0].max().item())],
+           "note": "wall between events: host glue (grouping, GrainSet, PeakTable) included"}
+    if cpu:
+        from oracle import oracle as orcm
+        ref = orcm.Reference() if orcm.have_reference() else orcm.Oracle()
+        chk = {"kind": "reference" if isinstance(ref, orcm.Reference) else "port"}
+        gv_h = gv.cpu().numpy()
+        # compute_gv on 1M peaks (the reference C from the same lab positions)
+        xyz_h = xyz[:1_000_000].cpu().numpy()
+        rgv = ref.compute_gv(xyz_h, ps.omega[:1_000_000], truth["omegasign"],
+                             truth["wavelength"], truth["wedge"], truth["chi"], t_arr)
+        chk["compute_gv_1M_max_abs_err"] = float(np.abs(rgv - gv_h[:1_000_000]).max())
+        # score() of 256 trials over every peak
+        rc = ref.score_many(trials[:256], gv_h, [tol])
+        chk["trial_counts_identical_256"] = bool(np.array_equal(rc, cbuf[:256].cpu().numpy()))
+        # the reference's sequential score_and_assign of all grains on 100k peaks
+        # (each peak's outcome depends on that peak alone)
+        sel = np.sort(np.random.default_rng(SEED + 14).choice(n, 100_000, replace=False))
+        rd = np.full(len(sel), 2.0)
+        rl = np.full(len(sel), -1, np.int32)
+        ref.assign_seq(u_ref, np.ascontiguousarray(gv_h[sel]), tol, rd, rl)
+        chk["assign_labels_identical_100k"] = bool(np.array_equal(rl, lab.cpu().numpy()[sel]))
+        chk["assign_drlv2_identical_100k"] = bool(np.array_equal(rd, d2.cpu().numpy()[sel]))
+        # 5 score_and_refine rounds of 64 grains on the same grouped peaks
+        order = state["order"].cpu().numpy()
+        off = state["off"].cpu().numpy()
+        k = 64
+        gsub = np.ascontiguousarray(gv_h[order[:off[k]]])
+        ru, rn, _ = ref.refine_csr(u_ref[:k], gsub, off[:k + 1], tol, rounds)
+        gu = state["grains"].ubis.view(-1, 3, 3)[:k].cpu().numpy()
+        gn = state["grains"].npk[:k].cpu().numpy()
+        scale = np.abs(ru).max(axis=(1, 2))
+        chk["refine_64_npk_identical"] = bool(np.array_equal(gn, rn))
+        chk["refine_64_ubi_max_rel_err"] = float((np.abs(gu - ru).max(axis=(1, 2)) / scale).max())
+        chk["all_identical"] = bool(chk["trial_counts_identical_256"] and
+                                    chk["assign_labels_identical_100k"] and
+                                    chk["assign_drlv2_identical_100k"] and
+                                    chk["refine_64_npk_identical"] and
+                                    chk["refine_64_ubi_max_rel_err"] <= 1e-9)
+        res["vs_reference"] = chk
+    return res
 
 
 def workload(rank=0, n_ubi=N_UBI):
@@ -589,7 +654,8 @@ def cuda_time_ms(torch, fn, steps, flush=None):
 
 def cpu_reference_rate(ps, ubis, seconds=10.0, kind="reference"):
     """The reference's own C score() over UBIs (OpenMP, all host threads) on a
-    bounded sample of the workload; pairs/s."""
+    bounded sample of the workload: (pairs/s record, the sample's counts
+    (m, T) for the first m UBIs)."""
     from oracle import oracle as orc
     lib = orc.Reference() if (kind == "reference" and orc.have_reference()) else orc.Oracle()
     kind = "reference" if isinstance(lib, orc.Reference) else "port"
@@ -602,11 +668,92 @@ def cpu_reference_rate(ps, ubis, seconds=10.0, kind="reference"):
     dt = time.perf_counter() - t0
     m = int(min(len(ubis), max(k, k * seconds / max(dt, 1e-3))))
     t0 = time.perf_counter()
-    lib.score_many(ubis[:m], gv, TOLS)
+    counts = lib.score_many(ubis[:m], gv, TOLS)
     dt = time.perf_counter() - t0
     pairs = m * len(gv) * len(TOLS)
-    return {"value": pairs / dt, "unit": "pairs/s", "cores": cores, "kind": kind,
-            "sample": "%d UBIs x %d g x %d tols (%.1f s)" % (m, len(gv), len(TOLS), dt)}
+    return ({"value": pairs / dt, "unit": "pairs/s", "cores": cores, "kind": kind,
+             "sample": "%d UBIs x %d g x %d tols (%.1f s)" % (m, len(gv), len(TOLS), dt)},
+            counts)
+
+
+def count_launches(torch, fn):
+    """Kernels launched by one call of fn, from the CUDA profiler's activity
+    record (memsets and copies excluded); None when profiling is unavailable."""
+    try:
+        from torch.profiler import ProfilerActivity, profile
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            fn()
+            torch.cuda.synchronize()
+        names = [e.name for e in prof.events()
+                 if str(getattr(e, "device_type", "")).endswith("CUDA")]
+        kernels = [nm for nm in names if not any(w in nm.lower() for w in
+                                                 ("memset", "memcpy", "memcpyasync"))]
+        return len(kernels), sorted(set(k.split("(")[0][:60] for k in kernels))
+    except Exception as e:  # noqa: BLE001  (the profiler is optional here)
+        return None, [repr(e)[:200]]
+
+
+def cfg0_measure(cpu=True, reps=3):
+    """Plain FP64 method, small: 50 FCC Al grains (|g| <= 1.0, 10% noise
+    peaks), compute_gv over every peak in FP64, then 3 score_and_refine
+    iterations at tol 0.05 for each of the 50 true UBIs perturbed by 0.1 deg and
+    0.1% strain -- through the drop-in module (imaged11_b200.cImageD11) with
+    host numpy buffers, one call at a time as an unchanged refinegrains caller
+    makes them, timed on the host clock; beside it the same call sequence on
+    the reference's compiled C."""
+    from imaged11_b200 import cImageD11 as cim, synth
+    ps = synth.simulate(50, "Al", gmax=1.0, seed=SEED + 21, noise_frac=0.10)
+    rng = np.random.default_rng(SEED + 22)
+    u0 = synth.perturb_ubis(ps.ubis, 0.1, 0.001, rng)
+    geo = ps.geo
+    xyz = np.ascontiguousarray(ps.xyz)
+    om = np.ascontiguousarray(ps.omega)
+    args = (geo["omegasign"], geo["wavelength"], geo["wedge"], geo["chi"])
+
+    def run_dropin():
+        gv = np.empty_like(xyz)
+        cim.compute_gv(xyz, om, *args, [0.0, 0.0, 0.0], gv)
+        out = []
+        for u in u0:
+            uu = np.array(u, order="C")
+            for _ in range(3):
+                n, d = cim.score_and_refine(uu, gv, 0.05)
+            out.append((uu, n, d))
+        return gv, out
+
+    run_dropin()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        gv, res = run_dropin()
+    ms = (time.perf_counter() - t0) / reps * 1e3
+    out = {"grains": 50, "peaks": int(len(xyz)), "iterations": 3, "tol": 0.05,
+           "calls_per_run": 1 + 3 * 50, "dropin_ms": ms,
+           "note": "host numpy buffers through the drop-in module, host clock"}
+    if cpu:
+        from oracle import oracle as orcm
+        ref = orcm.Reference() if orcm.have_reference() else orcm.Oracle()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            rgv = ref.compute_gv(xyz, om, *args, np.zeros(3))
+            rres = []
+            for u in u0:
+                uu = np.array(u, order="C")
+                for _ in range(3):
+                    n, d, uu = ref.score_and_refine(uu, rgv, 0.05)
+                rres.append((uu, n, d))
+        rms = (time.perf_counter() - t0) / reps * 1e3
+        scale = np.abs(np.asarray([r[0] for r in rres])).max(axis=(1, 2))
+        out["reference_ms"] = rms
+        out["reference_kind"] = "reference" if isinstance(ref, orcm.Reference) else "port"
+        out["vs_reference"] = {
+            "gv_max_abs_err": float(np.abs(gv - rgv).max()),
+            "npk_identical": bool(all(a[1] == b[1] for a, b in zip(res, rres))),
+            "ubi_max_rel_err": float(max(np.abs(a[0] - b[0]).max() / s
+                                         for a, b, s in zip(res, rres, scale))),
+            "mean_drlv2_max_rel_err": float(max(abs(a[2] - b[2]) / max(abs(b[2]), 1e-300)
+                                                for a, b in zip(res, rres)))}
+    return out
 
 
 def run_reference(args, rank, world):
@@ -667,6 +814,9 @@ def run_ours(args, rank, world, local_rank):
                 print(json.dumps(grid_measure(torch, dev, ps, ubis, steps=args.steps, cell=cell,
                                               xsub=xsub)))
         return 0
+    if args.case == "cfg0":     # the small drop-in sequence with host buffers
+        print(json.dumps(cfg0_measure()))
+        return 0
     if args.case == "translations":  # per-grain translation refinement
         print(json.dumps(translations_measure(torch, dev, steps=args.steps)))
         return 0
@@ -679,36 +829,35 @@ def run_ours(args, rank, world, local_rank):
         return 0
     n, m, T = len(ps.gv), len(ubis), len(TOLS)
     pairs = m * n * T
-
     gv_d = torch.tensor(ps.gv, device=dev)
     ubis_d = torch.tensor(ubis, device=dev)
-    gs = batch.GvecSet(gv_d)
-    ws = batch.BatchWorkspace(m, n, refine=False)
-    counts = torch.empty((m, T), dtype=torch.int32, device=dev)
     flush_buf = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
     def flush():
         flush_buf.fill_(1)
 
-    def step():
-        gs.prepare()
-        batch.score_batch(ubis_d, gs, TOLS, workspace=ws, out=counts)
-
-    # launch shape from the autotuner (untimed setup; counts do not depend on it)
     from imaged11_b200 import tune
-    gs.prepare()
-    tile, tune_table = tune.tune_score(ubis_d, gs, TOLS, reps=2)
+    # --- headline: exact batched scoring through the reciprocal-space cell
+    # index, binned join (index shape from the autotuner: untimed setup)
+    shape, grid_table = tune.tune_grid(ubis_d, gv_d, TOLS, cell_factors=(0.8, 1.0, 1.25),
+                                       xsubs=(4, 8), reps=2, method="bins")
+    base = batch.GvecGrid(gv_d, xsub=1)
+    grid = batch.GvecGrid(gv_d, cell=base.cs * shape[0], xsub=shape[1])
+    del base
+    ws = batch.BinsWorkspace(m, grid, batch.bins_box_estimate(ubis_d, grid, max(TOLS)))
+    counts = torch.empty((m, T), dtype=torch.int32, device=dev)
 
-    # correctness spot-check against the plain FP64 kernel (same assignments)
+    def step():
+        grid.refresh()      # the index rebuilt from the g-vectors every step
+        batch.score_grid(ubis_d, grid, TOLS, workspace=ws, out=counts, method="bins")
+
     step()
-    c64 = batch.score_many_fp64(ubis_d[:512], gs, TOLS)
-    assert torch.equal(c64, counts[:512]), "FP32+recheck counts differ from FP64"
     if args.kernel_only:        # profiling case: warm-up + timed steps, nothing else
         for _ in range(args.warmup):
             step()
         kt = cuda_time_ms(torch, step, args.steps, flush)
         torch.cuda.synchronize()
-        print(json.dumps({"case": "score_batch", "ubis": m, "gvectors": n, "tile": tile,
+        print(json.dumps({"case": "score_grid_bins", "ubis": m, "gvectors": n,
                           "ms_per_step": sum(kt) / len(kt),
                           "pairs_per_s": pairs / (sum(kt) / len(kt) * 1e-3)}))
         return 0
@@ -730,22 +879,54 @@ def run_ours(args, rank, world, local_rank):
     total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
     value = pairs * world / (ms_per_step * 1e-3)
+    gstats = grid.stats()
 
-    # the screening kernel alone (score_batch on prepared g-vectors)
-    k_times = cuda_time_ms(torch, lambda: batch.score_batch(ubis_d, gs, TOLS, workspace=ws,
-                                                           out=counts), max(2, args.steps), flush)
+    # the join kernel alone: CUDA events around its launches, recorded on the
+    # launching stream by the library, over the same steps
+    join_ms = []
+    st_ = torch.cuda.current_stream()
+    for _ in range(args.steps):
+        flush()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st_)
+        e1.record(st_)  # creates both events
+        batch.lib.id11b_grid_bins_time_join(e0.cuda_event, e1.cuda_event)
+        step()
+        e1.synchronize()
+        join_ms.append(e0.elapsed_time(e1))
+    join_ms = float(np.mean(join_ms))
+    launches, launch_names = count_launches(torch, step)
+
+    # plain FP64 kernel (reference arithmetic): every tolerance in one pass and
+    # one launch per tolerance, on the same 20,000 UBIs; counts compared
+    gs = batch.GvecSet(gv_d)
+    c64 = batch.score_many_fp64(ubis_d, gs, TOLS)
+    p64_fused = cuda_time_ms(torch, lambda: batch.score_many_fp64(ubis_d, gs, TOLS, out=c64),
+                             2, flush)
+    p64_per_tol = cuda_time_ms(torch, lambda: [batch.score_many_fp64(ubis_d, gs, [t_])
+                                               for t_ in TOLS], 1, flush)
+    rate64f = pairs / (np.mean(p64_fused) * 1e-3)
+    rate64 = pairs / (np.mean(p64_per_tol) * 1e-3)
+    same64 = bool(torch.equal(c64, counts))
+
+    # FP32 screening kernel (every pair tested, proven FP64 recheck band)
+    sws = batch.BatchWorkspace(m, n, refine=False)
+    gs.prepare()
+    tile, tune_table = tune.tune_score(ubis_d, gs, TOLS, reps=2)
+    c32 = torch.empty((m, T), dtype=torch.int32, device=dev)
+    batch.score_batch(ubis_d, gs, TOLS, workspace=sws, out=c32)
+    k_times = cuda_time_ms(torch, lambda: batch.score_batch(ubis_d, gs, TOLS, workspace=sws,
+                                                           out=c32), max(2, args.steps), flush)
     k_ms = float(np.mean(k_times))
-    nrecheck, nfallback = ws.stats()
+    nrecheck, nfallback = sws.stats()
+    same32 = bool(torch.equal(c32, counts))
 
-    # plain FP64 baseline: reference arithmetic, one launch per tolerance as
-    # the reference API scores one tolerance per call, and all tols at once
-    m64 = min(m, 2000)
-    p64_per_tol = cuda_time_ms(torch, lambda: [batch.score_many_fp64(ubis_d[:m64], gs, [t])
-                                               for t in TOLS], 2, flush)
-    p64_fused = cuda_time_ms(torch, lambda: batch.score_many_fp64(ubis_d[:m64], gs, TOLS), 2,
-                             flush)
-    rate64 = m64 * n * T / (np.mean(p64_per_tol) * 1e-3)
-    rate64f = m64 * n * T / (np.mean(p64_fused) * 1e-3)
+    # the lookup scorer on the same index (per-box lookups, FP64 candidates)
+    cw = batch.score_grid(ubis_d, grid, TOLS, method="walk")
+    w_times = cuda_time_ms(torch, lambda: batch.score_grid(ubis_d, grid, TOLS, method="walk",
+                                                          out=cw), max(2, args.steps), flush)
+    same_walk = bool(torch.equal(cw, counts))
 
     # compute_gv (HBM-bound FP64 streaming kernel), 10M peaks
     gv_gbs, gv_ms = compute_gv_measure(torch, ps, dev, 10_000_000, max(3, args.steps), flush)
@@ -773,23 +954,19 @@ def run_ours(args, rank, world, local_rank):
                                 cpu=(world == 1))
     adj = adjoint_measure(torch, dev, steps=max(3, args.steps))
     trans = translations_measure(torch, dev, steps=max(3, args.steps), cpu=(world == 1))
-    # the same scoring through the reciprocal-space cell index (exact FP64 lookups),
-    # index shape from the autotuner (untimed setup)
-    grid_shape, grid_table = tune.tune_grid(ubis_d, gs.gv, TOLS, reps=2)
-    cell = grid_measure(torch, dev, ps, ubis, steps=max(3, args.steps), flush=flush,
-                        check_counts=counts)
-    cell["tuned_shape"] = {"cell_factor": grid_shape[0], "xsub": grid_shape[1]}
-    cell["tuning_ms"] = {"%g,%d" % t: round(ms, 3) for t, ms in grid_table}
-    cell["ratio_vs_fp32_screening"] = cell["value"] / value
-    cell["ratio_vs_plain_fp64_all_tols"] = cell["value"] / rate64f
+    # the full-scale scan (cfg4) and the small drop-in sequence (cfg0)
+    pipe = pipeline_measure(torch, dev, cpu=(world == 1))
+    cfg0 = cfg0_measure(cpu=(world == 1))
 
     # end to end through the public API: pinned host inputs -> counts on host
     gv_h = torch.tensor(ps.gv).pin_memory()
     ub_h = torch.tensor(ubis).pin_memory()
+    ews = batch.BinsWorkspace(m, grid, ws.boxes)
 
     def e2e_step():
-        g = batch.GvecSet(gv_h.to(dev, non_blocking=True))
-        c = batch.score_batch(ub_h.to(dev, non_blocking=True), g, TOLS, workspace=ws)
+        g = batch.GvecGrid(gv_h.to(dev, non_blocking=True), cell=grid.cs, xsub=grid.xsub)
+        c = batch.score_grid(ub_h.to(dev, non_blocking=True), g, TOLS, workspace=ews,
+                             method="bins")
         return c.cpu()
 
     for _ in range(2):
@@ -808,42 +985,80 @@ def run_ours(args, rank, world, local_rank):
     sm_mhz = clocks["sm_mhz"] or 1965.0
     nsm = torch.cuda.get_device_properties(dev).multi_processor_count
     fp32_peak = nsm * 128 * 2 * sm_mhz * 1e6 / 1e12
-    achieved = (m * n * FLOP_PER_EVAL) / (k_ms * 1e-3) / 1e12
-    cpu = cpu_reference_rate(ps, ubis) if world == 1 else None
+    screened = gstats["pairs_screened"]
+    achieved = screened * FLOP_PER_EVAL / (join_ms * 1e-3) / 1e12
+    achieved32 = (m * n * FLOP_PER_EVAL) / (k_ms * 1e-3) / 1e12
+    cpu, ref_counts = cpu_reference_rate(ps, ubis) if world == 1 else (None, None)
+    parity = {"cfg1": {
+        "vs": "the reference's own score() (oracle/_ref, the unmodified src/closest.c)",
+        "ubis_checked": int(len(ref_counts)) if ref_counts is not None else 0,
+        "counts_identical": bool(np.array_equal(
+            counts[:len(ref_counts)].cpu().numpy(), ref_counts))
+        if ref_counts is not None else None,
+        "counts_equal_plain_fp64_all_ubis": same64,
+        "counts_equal_fp32_screening_all_ubis": same32,
+        "counts_equal_lookup_scorer_all_ubis": same_walk}}
+    if "vs_reference" in pipe:
+        parity["cfg4"] = pipe["vs_reference"]
+    if "vs_reference" in cfg0:
+        parity["cfg0"] = cfg0["vs_reference"]
     line = {
         "metric": "assigned peak x grain pairs/s", "value": value, "unit": "pairs/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64recheck", "data": "synthetic",
-        "config": dict(config_dict(n, m), tile={"ubis_per_thread": tile[0], "gsplit": tile[1]}),
-        "tuning_ms": {"%d,%d" % t: round(ms, 3) for t, ms in tune_table},
+        "config": dict(config_dict(n, m),
+                       method="exact batched scoring through the reciprocal-space cell index "
+                              "(binned join: FP32 screening of (UBI, hkl) boxes against the "
+                              "g of their cell rows, proven FP64 recheck band); the index is "
+                              "rebuilt from the g-vectors in every step",
+                       index_shape={"cell_factor": shape[0], "xsub": shape[1],
+                                    "cell_A^-1": grid.cs, "nx": grid.nx}),
+        "tuning_ms": {"%g,%d" % t_: round(ms, 3) for t_, ms in grid_table},
         "e2e": {"value": e2e_value, "unit": "pairs/s",
                 "h2d_bytes_per_step": int(ps.gv.nbytes + ubis.nbytes),
                 "d2h_bytes_per_step": int(m * T * 4)},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                     "traffic": K_BATCH_DRAM_BYTES,
-                     "traffic_note": "dram__bytes_read.sum + write.sum of one k_batch launch "
-                                     "captured with 2,048 UBIs (profiles/); the g tiles come "
-                                     "from L2 after their first read, so the DRAM bytes do not "
-                                     "grow with the UBI count",
-                     "kernel": "k_batch<%d,3,score>" % tile[0],
+                     "traffic": K_JOIN_DRAM_BYTES,
+                     "traffic_note": K_JOIN_TRAFFIC_NOTE,
+                     "kernel": "k_join<3> (binned join)",
+                     "join_ms": join_ms, "pairs_screened": screened,
                      "peak_note": "CUDA-core FP32 = SMs x 128 x 2 x median SM clock under load; "
-                                  "%d FLOP per (UBI,g) evaluation" % FLOP_PER_EVAL},
-        "plain_fp64": {"value_per_tol_launch": rate64, "value_all_tols": rate64f,
-                       "unit": "pairs/s", "ubis": m64,
-                       "ratio_vs_per_tol": value / rate64, "ratio_vs_all_tols": value / rate64f},
-        "cell_index": cell,
+                                  "%d FLOP per screened (box, g) pair" % FLOP_PER_EVAL},
+        "gpu_launches": None if launches is None else launches * args.steps,
+        "gpu_launches_note": "kernels one step launches (CUDA profiler activity record) x steps",
+        "gpu_kernels": launch_names,
+        "plain_fp64": {"value_all_tols": rate64f, "value_per_tol_launch": rate64,
+                       "unit": "pairs/s", "ubis": m, "ms_all_tols": float(np.mean(p64_fused)),
+                       "ratio_vs_plain_fp64_all_tols": value / rate64f,
+                       "ratio_vs_plain_fp64_per_tol_launch": value / rate64,
+                       "counts_equal": same64},
+        "fp32_screening": {"value": pairs / (k_ms * 1e-3), "ms": k_ms,
+                           "tile": {"ubis_per_thread": tile[0], "gsplit": tile[1]},
+                           "roofline": {"bound": "fp32", "achieved": achieved32,
+                                        "peak": fp32_peak, "frac": achieved32 / fp32_peak,
+                                        "kernel": "k_batch<%d,3,score>" % tile[0]},
+                           "recheck": {"fp64_pairs": nrecheck, "fraction": nrecheck / (m * n),
+                                       "fallback_ubis": nfallback},
+                           "counts_equal": same32},
+        "cell_index_lookup": {"value": pairs / (float(np.mean(w_times)) * 1e-3),
+                              "ms": float(np.mean(w_times)), "counts_equal": same_walk},
+        "cell_index": {"fp64_rechecks": gstats["pairs_tested"],
+                       "pairs_screened_fp32": screened,
+                       "screened_fraction_of_all_pairs": screened / float(m * n),
+                       "plain_scan_ubis": gstats["fallback_ubis"],
+                       "boxes_capacity": ws.boxes},
+        "parity": parity,
         "refine_csr": refine,
         "adjoint": adj,
         "translations": trans,
+        "pipeline": pipe,
+        "cfg0": cfg0,
         "compute_gv": {"peaks": 10_000_000, "ms": gv_ms, "achieved_gbs": gv_gbs,
                        "cpu_baseline": gv_cpu,
                        "peak_gbs": hbm_peak, "peak_kind": hbm_kind,
                        "frac": gv_gbs / hbm_peak, "bytes_per_peak": 56},
-        "recheck": {"fp64_pairs": nrecheck, "fraction": nrecheck / (m * n),
-                    "fallback_ubis": nfallback},
-        "gpu_launches": 4 * args.steps,
         "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "cpu_baseline": cpu,
     }
@@ -862,7 +1077,7 @@ def main():
                     help="only warm-up + timed steps of the scoring step (profiling case)")
     ap.add_argument("--case", default="score",
                     choices=["score", "gv", "geometry", "grid", "translations", "refine", "adjoint",
-                             "pipeline"],
+                             "pipeline", "cfg0"],
                     help="gv: compute_gv alone on --peaks lab positions; refine: per-grain "
                          "CSR refinement alone (profiling cases)")
     ap.add_argument("--peaks", type=int, default=10_000_000)

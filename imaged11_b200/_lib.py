@@ -62,7 +62,8 @@ _SIGNATURES = [
     ("id11b_grid_score_workspace_bytes", _i64, [_i64, _i]),
     ("id11b_dev_score_grid", _i, [_p, _i64, _p, _i64, _i, _i, _p, _p, _i, _p, _p, _p, _i64,
                                    _p]),
-    ("id11b_grid_stats", _i, [_p, _p, _p, _p, _p, _p]),
+    ("id11b_grid_stats", _i, [_p, _p, _p, _p, _p, _p, _p]),
+    ("id11b_grid_bins_time_join", _i, [_p, _p]),
     ("id11b_grid_bins_workspace_bytes", _i64, [_i64, _i, _i, _i64]),
     ("id11b_dev_score_grid_bins", _i, [_p, _i64, _p, _i64, _i, _i, _p, _p, _i, _p, _p, _p,
                                         _i64, _p]),

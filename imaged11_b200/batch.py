@@ -175,15 +175,24 @@ class GvecGrid:
                                        self.cs, self.nx, self.xsub, self.buf.data_ptr(), nbytes,
                                        _stream()), "build_grid")
 
+    def refresh(self):
+        """Rebuild the index from self.gv (changed in place) into the same
+        buffer and shape, reading nothing back: every g must stay inside the
+        cube the index was sized for (|g_j| <= gmax; larger or non-finite g go
+        to the list of g outside the regular range, as at build)."""
+        check(lib.id11b_dev_build_grid(self.gv.data_ptr(), self.n, self.gmax, self.rmax,
+                                       self.cs, self.nx, self.xsub, self.buf.data_ptr(),
+                                       self.buf.numel(), _stream()), "build_grid")
+
     def stats(self):
         """dict: regular / listed g-vectors; UBIs scanned plainly and pairs
         evaluated by the last score_grid call (synchronises)."""
         import ctypes
-        v = [ctypes.c_int64(0) for _ in range(4)]
+        v = [ctypes.c_int64(0) for _ in range(5)]
         check(lib.id11b_grid_stats(self.buf.data_ptr(), *[ctypes.addressof(x) for x in v],
                                    _stream()), "grid_stats")
-        return dict(zip(("regular", "special", "fallback_ubis", "pairs_tested"),
-                        (x.value for x in v)))
+        return dict(zip(("regular", "special", "fallback_ubis", "pairs_tested",
+                         "pairs_screened"), (x.value for x in v)))
 
 
 BINS_TOL_LIMIT = 0.4   # the binned join takes tolerances below this

@@ -29,6 +29,7 @@ struct Header {
     int32_t nxx;
     unsigned long long nfallback;  // UBIs scored by the plain scan (last call)
     unsigned long long ntested;    // (UBI, g) pairs evaluated in FP64 (last call)
+    unsigned long long npairs;     // (box, g) pairs screened in FP32 (last binned call)
 };
 
 struct Tols {

@@ -575,6 +575,7 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
     const Staged T{s_gx, s_gy, s_gz, s_gp};
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned ntest = 0;
+    unsigned long long npairs = 0;  // lane 0: (box, g) pairs screened
     for (;;) {
         if (threadIdx.x == 0) s_row = atomicAdd(&info->next_row, 1);
         __syncthreads();
@@ -720,6 +721,8 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
                     const int nrun = min(32, nb - k0);
                     const int ga = s_gs[max(box_fx(s_box[k0]) - P.Rx, gxa) - gxa];
                     const int gb = s_gs[min(box_fx(s_box[k0 + nrun - 1]) + P.Rx, gxb) - gxa + 1];
+                    if (lane == 0 && ga < gb)
+                        npairs += (unsigned long long)nrun * (unsigned)(((gb + 1) & ~1) - (ga & ~1));
                     if (lane < nrun && ga < gb) {
                         const uint64_t rec = s_box[k0 + lane];
                         const int64_t ubi = P.i0 + (int64_t)(rec >> 44);
@@ -758,6 +761,7 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
     }
     const long long tt = warp_sum((long long)ntest);
     if (lane == 0 && tt) atomicAdd(&Hp->ntested, (unsigned long long)tt);
+    if (lane == 0 && npairs) atomicAdd(&Hp->npairs, npairs);
 }
 
 // UBIs outside the binned path's limits: exact FP64 over every regular g, one
@@ -914,6 +918,19 @@ float float_ru(double x) {
 using namespace id11b::grid;
 using namespace id11b::grid::bins;
 
+namespace {
+// events that bracket the join launches of the calling thread's next binned
+// call (a measurement hook; cleared by that call)
+thread_local cudaEvent_t t_join_start = nullptr, t_join_stop = nullptr;
+}  // namespace
+
+extern "C" int id11b_grid_bins_time_join(void* start_event, void* stop_event) {
+    if ((start_event == nullptr) != (stop_event == nullptr)) return ID11B_ERR_ARG;
+    t_join_start = (cudaEvent_t)start_event;
+    t_join_stop = (cudaEvent_t)stop_event;
+    return ID11B_OK;
+}
+
 extern "C" int64_t id11b_grid_bins_workspace_bytes(int64_t m, int32_t nx, int32_t xsub,
                                                    int64_t boxes) {
     if (m < 0 || !grid_dims_ok(nx, xsub) || boxes < 0) return -1;
@@ -978,7 +995,7 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     int* tot = (int*)(w + B.tot);
     uint64_t* tmp = (uint64_t*)(w + B.tmp);
     uint64_t* recs = (uint64_t*)(w + B.recs);
-    ID11B_CHECK(cudaMemsetAsync(&H->nfallback, 0, 2 * sizeof(unsigned long long), st));
+    ID11B_CHECK(cudaMemsetAsync(&H->nfallback, 0, 3 * sizeof(unsigned long long), st));
     if (m == 0) return ID11B_OK;
     ID11B_CHECK(cudaMemsetAsync(counts, 0, sizeof(int32_t) * (size_t)(m * ntol), st));
     if (sums) ID11B_CHECK(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)(m * ntol), st));
@@ -1062,6 +1079,9 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
                          4 * sizeof(int) * (size_t)(std::max(nxx, nhalo) + 1) +
                          2 * sizeof(int) * (size_t)(nhalo + 1);
     const int jgrid = num_sms() * ID11B_BINS_DISPATCH(join_ctas, jsmem);
+    cudaEvent_t ev0 = t_join_start, ev1 = t_join_stop;
+    t_join_start = t_join_stop = nullptr;
+    bool ev0_done = false;
     for (size_t c = 0; c + 1 < cuts.size() && bi.total > 0; c++) {
         const int64_t i0 = cuts[c], mc = cuts[c + 1] - cuts[c];
         if (cuts.size() > 2) {
@@ -1081,9 +1101,17 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
         ID11B_CHECK_LAUNCH();
         ID11B_CHECK(cudaMemsetAsync(&info->next_row, 0, sizeof(int), st));
         P.i0 = i0;
+        if (ev0 && !ev0_done) {
+            ID11B_CHECK(cudaEventRecord(ev0, st));
+            ev0_done = true;
+        }
         rc = ID11B_BINS_DISPATCH(launch_join, jgrid, jsmem, recs, rstart, nrows, nhalo, info,
                                  packs, ubis, H, start, gs, g4, P, counts, sums, st);
         if (rc) return rc;
+    }
+    if (ev1) {
+        if (!ev0_done) ID11B_CHECK(cudaEventRecord(ev0, st));
+        ID11B_CHECK(cudaEventRecord(ev1, st));
     }
     return ID11B_BINS_DISPATCH(launch_rest, ubis, m, fallback, bi.nfallback, H, start, gs, gv,
                                (const int*)(g + L.spec), (const int*)(g + L.spos) + n,

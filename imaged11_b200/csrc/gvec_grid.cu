@@ -933,7 +933,7 @@ extern "C" int id11b_dev_score_grid(const double* ubis, int64_t m, const double*
     const Layout L = layout(n, (int64_t)nx * nx * nx * xsub);
     char* b = (char*)gridbuf;
     Header* H = (Header*)b;
-    ID11B_CHECK(cudaMemsetAsync(&H->nfallback, 0, 2 * sizeof(unsigned long long), st));
+    ID11B_CHECK(cudaMemsetAsync(&H->nfallback, 0, 3 * sizeof(unsigned long long), st));
     if (m == 0) return ID11B_OK;
     const int parts = score_parts(m);
     const int64_t items = (m * parts + m) * ntol;
@@ -963,7 +963,8 @@ extern "C" int id11b_dev_score_grid(const double* ubis, int64_t m, const double*
 }
 
 extern "C" int id11b_grid_stats(const void* gridbuf, int64_t* nregular, int64_t* nspecial,
-                                int64_t* nfallback, int64_t* ntested, void* stream) {
+                                int64_t* nfallback, int64_t* ntested, int64_t* npairs,
+                                void* stream) {
     if (!gridbuf) return ID11B_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     Header h;
@@ -980,6 +981,7 @@ extern "C" int id11b_grid_stats(const void* gridbuf, int64_t* nregular, int64_t*
     if (nspecial) *nspecial = ns;
     if (nfallback) *nfallback = (int64_t)h.nfallback;
     if (ntested) *ntested = (int64_t)h.ntested;
+    if (npairs) *npairs = (int64_t)h.npairs;
     return ID11B_OK;
 }
 

@@ -153,26 +153,38 @@ def grid_key(n):
     return "grid|%s|%d" % (_device_name(), _bucket(n))
 
 
-def tune_grid(ubis, gv, tols, cell_factors=(0.8, 1.0, 1.25), xsubs=(1, 2, 4, 8), reps=2):
+def tune_grid(ubis, gv, tols, cell_factors=(0.8, 1.0, 1.25), xsubs=(1, 2, 4, 8), reps=2,
+              method=None):
     """Time score_grid on these inputs for cell-index shapes: y/z cell side =
     factor x the default (about one g per cell of the bounding cube) and x cut
     xsub times finer; cache the fastest per g-count bucket (GvecGrid uses it
-    when built without explicit shape) and return ((factor, xsub), table)."""
+    when built without explicit shape) and return ((factor, xsub), table).
+    method: score_grid's method (None: its default for these tolerances)."""
     from . import batch
     torch = _torch()
     g = batch._dev(gv, torch.float64).reshape(-1, 3)
     u = batch._dev(ubis, torch.float64).reshape(-1, 9)
     base = batch.GvecGrid(g, xsub=1)
-    out = torch.empty((u.shape[0], len(batch._tols(tols))), dtype=torch.int32, device=g.device)
+    t = batch._tols(tols)
+    out = torch.empty((u.shape[0], len(t)), dtype=torch.int32, device=g.device)
     table = []
     for f in cell_factors:
         for xs in xsubs:
             grid = batch.GvecGrid(g, cell=base.cs * f, xsub=xs)
             if grid.xsub != xs:
                 continue  # over the cell budget
-            ms = _time(lambda: batch.score_grid(u, grid, tols, out=out), reps)
+            m = method
+            if m is None:
+                m = "bins" if float(t.max()) < batch.BINS_TOL_LIMIT and batch.bins_fit(grid) \
+                    else "walk"
+            if m == "bins" and not batch.bins_fit(grid):
+                continue
+            ws = batch.BinsWorkspace(u.shape[0], grid, batch.bins_box_estimate(
+                u, grid, float(t.max()))) if m == "bins" else None
+            ms = _time(lambda: batch.score_grid(u, grid, t, out=out, method=m, workspace=ws),
+                       reps)
             table.append(((f, xs), ms))
-            del grid
+            del grid, ws
     best = min(table, key=lambda x: x[1])[0]
     _cache[grid_key(g.shape[0])] = list(best)
     _autosave()

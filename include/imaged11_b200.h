@@ -253,8 +253,8 @@ int id11b_dev_score_batch_tiled(const double *ubis, int64_t m, const double *gv,
  * arithmetic.  A UBI whose lookup would cost more than a plain scan
  * (non-finite, singular, condition number above 1e6, more candidate hkl
  * than g) is scored by a plain scan.  id11b_grid_stats reports the regular and
- * listed g, and for the last score call the UBIs scanned plainly and the pairs
- * evaluated. */
+ * listed g, and for the last score call the UBIs scanned plainly, the pairs
+ * evaluated in FP64 and (binned calls) the (box, g) pairs screened in FP32. */
 int id11b_dev_gvec_bounds(const double *gv, int64_t n, uint32_t *bounds, void *stream);
 int id11b_grid_plan(float gmax, int64_t n, double cell, int32_t *nx, double *cs);
 int64_t id11b_grid_bytes(int64_t n, int32_t nx, int32_t xsub);
@@ -267,7 +267,7 @@ int id11b_dev_score_grid(const double *ubis, int64_t m, const double *gv, int64_
                          int32_t *counts, double *sums, void *ws, int64_t ws_bytes,
                          void *stream);
 int id11b_grid_stats(const void *gridbuf, int64_t *nregular, int64_t *nspecial,
-                     int64_t *nfallback, int64_t *ntested, void *stream);
+                     int64_t *nfallback, int64_t *ntested, int64_t *npairs, void *stream);
 
 /* The same counts (and optional FP64 sums of the counted drlv2) as
  * id11b_dev_score_grid -- identical to the reference's score() for every
@@ -289,6 +289,10 @@ int id11b_grid_stats(const void *gridbuf, int64_t *nregular, int64_t *nspecial,
  * asked for, are added with double atomics: their last bits can differ
  * between runs; counts never do. */
 int64_t id11b_grid_bins_workspace_bytes(int64_t m, int32_t nx, int32_t xsub, int64_t boxes);
+/* Measurement hook: the calling thread's next id11b_dev_score_grid_bins call
+ * records start_event before its first join launch and stop_event after its
+ * last (both cudaEvent_t, created by the caller; NULL, NULL clears). */
+int id11b_grid_bins_time_join(void *start_event, void *stop_event);
 int id11b_dev_score_grid_bins(const double *ubis, int64_t m, const double *gv, int64_t n,
                               int32_t nx, int32_t xsub, const void *gridbuf,
                               const double *tols_host, int ntol, int32_t *counts, double *sums,

@@ -192,6 +192,7 @@ class Reference(_Lib):
         L = self.lib
         L.ref_score_many.argtypes = [_p, _i64, _p, _i64, _p, _i, _p]
         L.ref_refine_csr.argtypes = [_p, _p, _p, _i64, _d, _i, _p, _p]
+        L.ref_assign_seq.argtypes = [_p, _i64, _p, _i64, _d, _p, _p]
         L.ref_max_threads.restype = _i
         L.cimaged11_omp_set_num_threads.argtypes = [_i]
 
@@ -214,6 +215,16 @@ class Reference(_Lib):
         self.lib.ref_refine_csr(_ptr(u), _ptr(g), _ptr(off), ng, tol, iters,
                                 _ptr(npk), _ptr(d))
         return u.reshape(-1, 3, 3), npk, d
+
+    def assign_seq(self, ubis, gv, tol, drlv2, labels):
+        """score_and_assign of grains 0 .. m-1 in order on (drlv2, labels),
+        updated in place (float64 / int32 C arrays)."""
+        u = _c64(ubis).reshape(-1, 9)
+        g = _c64(gv).reshape(-1, 3)
+        assert drlv2.dtype == np.float64 and labels.dtype == np.int32
+        assert drlv2.flags.c_contiguous and labels.flags.c_contiguous
+        self.lib.ref_assign_seq(_ptr(u), len(u), _ptr(g), len(g), float(tol), _ptr(drlv2),
+                                _ptr(labels))
 
     def max_threads(self):
         return int(self.lib.ref_max_threads())

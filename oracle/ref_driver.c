@@ -20,6 +20,9 @@ typedef double vec[3];
 int score(vec ubi[3], vec gv[], double tol, int ng);
 void score_and_refine(vec ubi[3], vec gv[], double tol, int *n_arg,
                       double *sumdrlv2_arg, int ng);
+/* ImageD11 src/closest.c:366 */
+int score_and_assign(vec *ubi, vec *gv, double tol, double *drlv2, int *labels, int label,
+                     int ng);
 
 void ref_score_many(const double *ubis, int64_t m, const double *gv, int64_t ng,
                     const double *tols, int ntol, int32_t *counts) {
@@ -43,6 +46,15 @@ void ref_refine_csr(double *ubis, const double *gv, const int64_t *offsets,
         npk[g] = n;
         drlv2[g] = d;
     }
+}
+
+/* score_and_assign for grains 0 .. m-1 in order, as fight_over_peaks calls it
+   (ImageD11/indexing.py); the reference parallelises each call over the g. */
+void ref_assign_seq(const double *ubis, int64_t m, const double *gv, int64_t ng, double tol,
+                    double *drlv2, int32_t *labels) {
+    for (int64_t i = 0; i < m; i++)
+        score_and_assign((vec *)(ubis + 9 * i), (vec *)gv, tol, drlv2, (int *)labels, (int)i,
+                         (int)ng);
 }
 
 int ref_max_threads(void) {

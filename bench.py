@@ -212,17 +212,17 @@ def update_geometry_measure(torch, dev, n_peaks=10_000_000, steps=5, flush=None)
 
 def refine_workload(seed=SEED + 7, ngrains=2000):
     """Uneven per-grain refinement: hcp Ti grains (a=2.95, c=4.68 A), per-grain
-    peak counts log-uniform in 20..2000 set by a per-grain |g| cutoff (capped by
-    the reflections the 2048^2 detector can record, ~1,500 at |g|<=2.2), each
-    UBI 0.2 deg and 0.2% strain off its true value."""
+    peak counts log-uniform in 20..2000, each grain's shortest reflections up to
+    that count (a per-grain |g| cutoff) as g-vectors with 5e-4 1/A noise, no
+    detector; each UBI 0.2 deg and 0.2% strain off its true value.  (The stated
+    total of about 1.2M peaks does not follow from these numbers: counts
+    log-uniform over 20..2,000 have mean 430, so 2,000 grains hold about 0.86M.)"""
     from imaged11_b200 import synth
     rng = np.random.default_rng(seed)
     counts = np.exp(rng.uniform(np.log(20), np.log(2000), ngrains)).astype(int)
-    ps = synth.simulate(ngrains, "Ti_hcp", gmax=2.2, seed=seed, noise_frac=0.0,
-                        per_grain_counts=counts)
-    idx, off = ps.grain_offsets()
-    u0 = synth.perturb_ubis(ps.ubis, 0.2, 0.002, rng)
-    return np.ascontiguousarray(ps.gv[idx]), off, u0
+    gv, off, ubis = synth.grain_gvectors(counts, "Ti_hcp", rng)
+    u0 = synth.perturb_ubis(ubis, 0.2, 0.002, rng)
+    return gv, off, u0
 
 
 def refine_csr_measure(torch, dev, iters=5, tol=0.05, steps=5, flush=None, cpu=True):
@@ -264,6 +264,32 @@ def refine_csr_measure(torch, dev, iters=5, tol=0.05, steps=5, flush=None, cpu=T
            "value": pairs / (np.mean(times_g) * 1e-3), "unit": "pairs/s",
            "plain_fp64_value": pairs / (np.mean(times_p) * 1e-3)}
     out["ratio_vs_plain_fp64"] = out["value"] / out["plain_fp64_value"]
+    # compensated FP32 sums (FP32 screening, FP64 solves) against the FP64 sums
+    fp64_u = gs.ubis.clone()
+    reset()
+    graph.replay()
+    torch.cuda.synchronize()
+    fp64_u.copy_(gs.ubis)
+    fp64_n = gs.npk.clone()
+    t32 = []
+    for _ in range(steps + 1):
+        reset()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        gs.refine(tol, iters, precision="f32c")
+        e1.record(st)
+        e1.synchronize()
+        t32.append(e0.elapsed_time(e1))
+    u32 = gs.ubis.view(-1, 9)
+    scale64 = fp64_u.view(-1, 9).abs().max(1, keepdim=True).values.clamp_min(1e-300)
+    out["compensated_fp32"] = {
+        "ms": float(np.mean(t32[1:])), "value": pairs / (np.mean(t32[1:]) * 1e-3),
+        "npk_equal_fp64_sums": bool(torch.equal(gs.npk, fp64_n)),
+        "ubi_max_rel_diff_vs_fp64_sums": float(((u32 - fp64_u.view(-1, 9)).abs() /
+                                                scale64).max().item()),
+        "note": "FP32 screening with the proven band + compensated FP32 normal equations, "
+                "FP64 3x3 solves, one launch (not graph-captured)"}
     if cpu:
         from oracle import oracle as orc
         lib = orc.Reference() if orc.have_reference() else orc.Oracle()
@@ -293,6 +319,10 @@ def refine_csr_measure(torch, dev, iters=5, tol=0.05, steps=5, flush=None, cpu=T
     return out
 
 
+# the cfg4 scan's starting geometry: the truth offset by these amounts (um,
+# px, rad, deg)
+CFG4_START_OFFSETS = dict(distance=300., y_center=0.4, z_center=-0.3, tilt_y=4e-4,
+                          tilt_z=-3e-4, wedge=0.005)
 CFG3_TRUTH = dict(distance=152300., y_center=1024 + 3.7, z_center=1024 - 2.1, tilt_x=0.004,
                   tilt_y=-0.002, tilt_z=0.006, wedge=0.01, chi=0.02, t_x=5., t_y=-3., t_z=2.)
 
@@ -374,7 +404,7 @@ def adjoint_measure(torch, dev, steps=5, refine=True):
     nominal = dict(truth, distance=150000., y_center=1024., z_center=1024., tilt_x=0.,
                    tilt_y=0., tilt_z=0., wedge=0., chi=0., t_x=0., t_y=0., t_z=0.)
     p0 = adjoint.params_tensor(nominal)
-    u0 = adjoint.best_ubis(adjoint.gvectors(p0, peaks), peaks)
+    u0 = adjoint.best_ubis(p0, peaks)
 
     def grad_eval():
         p = p0.clone().requires_grad_(True)
@@ -382,14 +412,25 @@ def adjoint_measure(torch, dev, steps=5, refine=True):
         adjoint.loss(p, u, peaks).backward()
         return p.grad, u.grad
 
+    def projected_eval():
+        p = p0.clone().requires_grad_(True)
+        adjoint.projected_loss(p, peaks).backward()
+        return p.grad
+
     for _ in range(3):
         grad_eval()
+        projected_eval()
     times = cuda_time_ms(torch, grad_eval, steps)
+    tproj = cuda_time_ms(torch, projected_eval, steps)
     out = {"grains": peaks.ngrains, "peaks": peaks.n, "params": 12 + 9 * peaks.ngrains,
            "gradient_ms": float(np.mean(times)),
            "gradient_peaks_per_s": peaks.n / (np.mean(times) * 1e-3),
-           "note": "one residual forward + adjoint pass through torch.autograd, host "
-                   "geometry assembly included"}
+           "projected_gradient_ms": float(np.mean(tproj)),
+           "note": "gradient_ms: loss and its gradient in the 12 geometry parameters and "
+                   "the 500 x 9 UBI elements through torch.autograd (one fused residual + "
+                   "adjoint kernel, one reduction, geometry kept on the device); "
+                   "projected_gradient_ms: the same with every grain's UBI solved in "
+                   "closed form inside the kernel (one L-BFGS evaluation of refine_geometry)"}
     if refine:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -410,8 +451,9 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
     (binned join) -> batched score_and_assign of every peak to the 20,000
     grains (their UBIs 0.2 deg / 0.2% off truth) -> peaks grouped by label ->
     `rounds` rounds of per-grain refinement -> hkl of the assigned peaks from
-    the refined UBIs -> one geometry step (one L-BFGS iteration on the 12
-    geometry parameters, every grain's UBI re-solved, driven by the adjoint).
+    the refined UBIs -> a geometry step (3 L-BFGS iterations on the 12
+    geometry parameters, every grain's UBI re-solved in closed form inside the
+    adjoint kernel at each evaluation).
     Each stage's output is checked against the reference's own C on a sample
     (cpu=True): compute_gv on 1M peaks, score() of 256 trials over all peaks,
     the sequential score_and_assign of all 20,000 grains on 100k peaks, and 5
@@ -421,6 +463,10 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
     from imaged11_b200 import cImageD11 as cim
     from imaged11_b200._lib import lib, check
     truth = synth.default_geometry(**CFG3_TRUTH)
+    # the pipeline runs from the experiment's starting estimate of the
+    # geometry, a little off the truth the peaks were simulated with; the
+    # geometry step moves it towards the truth
+    est = dict(truth, **{k: truth[k] + d for k, d in CFG4_START_OFFSETS.items()})
     ng = 20000
     rng = np.random.default_rng(SEED + 13)
     cells = ["Ti_hcp" if x < 0.7 else "Ti_beta" for x in rng.random(ng)]
@@ -430,7 +476,7 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
     trials = np.concatenate([
         synth.trial_ubis(ps.ubis[np.array(cells) == c], int(n_ubi * frac), 0.1, 0.5, rng, cell=c)
         for c, frac in (("Ti_hcp", 0.7), ("Ti_beta", 0.3))])
-    p, r, dist = synth.xlylzl_params(truth)
+    p, r, dist = synth.xlylzl_params(est)
     s_d = torch.tensor(ps.s, device=dev)
     f_d = torch.tensor(ps.f, device=dev)
     om_d = torch.tensor(ps.omega, device=dev)
@@ -441,7 +487,7 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
     u_ref = synth.perturb_ubis(ps.ubis, 0.2, 0.002, rng)
     u_ref_d = torch.tensor(u_ref, device=dev)
     stream = torch.cuda.current_stream().cuda_stream
-    t_arr = np.array([truth["t_x"], truth["t_y"], truth["t_z"]])
+    t_arr = np.array([est["t_x"], est["t_y"], est["t_z"]])
     cbuf = torch.empty((len(trials), 1), dtype=torch.int32, device=dev)
     d2 = torch.empty(n, dtype=torch.float64, device=dev)
     lab = torch.empty(n, dtype=torch.int32, device=dev)
@@ -451,8 +497,8 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
     def run(ev, shape=None):
         ev[0].record()
         cim.compute_xlylzl(s_d, f_d, p, r.ravel(), dist, xyz)
-        check(lib.id11b_dev_compute_gv(xyz.data_ptr(), om_d.data_ptr(), truth["omegasign"],
-                                       truth["wavelength"], truth["wedge"], truth["chi"],
+        check(lib.id11b_dev_compute_gv(xyz.data_ptr(), om_d.data_ptr(), est["omegasign"],
+                                       est["wavelength"], est["wedge"], est["chi"],
                                        t_arr.ctypes.data, gv.data_ptr(), g4.data_ptr(), n,
                                        stream), "compute_gv")
         ev[1].record()
@@ -478,16 +524,21 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
         ub_pk = grains.ubis.view(-1, 3, 3).index_select(0, gl)
         hkl = torch.round(torch.einsum("nij,nj->ni", ub_pk, grains.gv))
         peaks = adjoint.PeakTable(s_d.index_select(0, order), f_d.index_select(0, order),
-                                  om_d.index_select(0, order), hkl, off, truth)
-        p0 = adjoint.params_tensor(truth)
-        p1, _, hist = adjoint.refine_geometry(peaks, p0, max_iter=1)
+                                  om_d.index_select(0, order), hkl, off, est)
+        p0 = adjoint.params_tensor(est)
+        p1, _, hist = adjoint.refine_geometry(peaks, p0, max_iter=3)
         ev[5].record()
         ev[5].synchronize()
+        moved = dict(zip(adjoint.PARAMS, p1.cpu().numpy()))
+        keys = ("distance", "y_center", "z_center", "tilt_y", "tilt_z", "wedge")
         out.update(assigned=int(n - first), refined_peaks=grains.peaks,
                    npk_median=int(grains.npk.median().item()),
-                   geometry_step={"loss_before": hist[0], "loss_after": min(hist),
+                   geometry_step={"loss_before": hist[0], "loss_after": hist[-1],
                                   "evaluations": len(hist),
-                                  "step_applied": bool(min(hist) <= hist[0])})
+                                  "loss_reduced": bool(hist[-1] < hist[0]),
+                                  "error_vs_truth_before": {k: est[k] - truth[k] for k in keys},
+                                  "error_vs_truth_after": {k: float(moved[k] - truth[k])
+                                                           for k in keys}})
         state.update(grid=grid, order=order, off=off, grains=grains)
 
     run([torch.cuda.Event(enable_timing=True) for _ in range(6)])   # warm-up (module loads)
@@ -534,8 +585,8 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
         gv_h = gv.cpu().numpy()
         # compute_gv on 1M peaks (the reference C from the same lab positions)
         xyz_h = xyz[:1_000_000].cpu().numpy()
-        rgv = ref.compute_gv(xyz_h, ps.omega[:1_000_000], truth["omegasign"],
-                             truth["wavelength"], truth["wedge"], truth["chi"], t_arr)
+        rgv = ref.compute_gv(xyz_h, ps.omega[:1_000_000], est["omegasign"],
+                             est["wavelength"], est["wedge"], est["chi"], t_arr)
         chk["compute_gv_1M_max_abs_err"] = float(np.abs(rgv - gv_h[:1_000_000]).max())
         # score() of 256 trials over every peak
         rc = ref.score_many(trials[:256], gv_h, [tol])
@@ -586,40 +637,67 @@ def config_dict(n, m):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons sampled every 20 ms by a reader
+    thread that stamps each sample on arrival; the sampler is live before the
+    timed region starts, and summary() keeps the samples taken inside it (or,
+    for a region shorter than one interval, the ones on either side)."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 20
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.samples = []   # (arrival time, line)
+        self.t0 = self.t1 = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            if line.strip():
+                self.samples.append((time.monotonic(), line))
 
     def __enter__(self):
+        import threading
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+            t_end = time.monotonic() + 10.0
+            while not self.samples and time.monotonic() < t_end and self.proc.poll() is None:
+                time.sleep(0.005)
         except OSError:
             self.proc = None
+        self.t0 = time.monotonic()
         return self
 
     def __exit__(self, *a):
-        self.lines = []
+        self.t1 = time.monotonic()
         if self.proc is not None:
+            time.sleep(2.5 * self.PERIOD_MS / 1e3)   # the sample that covers the end
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            self.reader.join(timeout=5)
 
     def summary(self):
+        inside = [l for t, l in self.samples
+                  if self.t0 is not None and self.t0 <= t <= self.t1 + self.PERIOD_MS / 1e3]
+        where = "inside the timed region"
+        if not inside and self.samples:
+            before = [l for t, l in self.samples if t < self.t0][-1:]
+            after = [l for t, l in self.samples if t > self.t1][:1]
+            inside = before + after
+            where = "the samples on either side of a timed region shorter than %d ms" % \
+                self.PERIOD_MS
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
+        for l in inside:
             f = [x.strip() for x in l.split(",")]
             if len(f) < 9:
                 continue
@@ -632,7 +710,8 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "sampled": where,
+                "window_ms": None if self.t0 is None else (self.t1 - self.t0) * 1e3}
 
 
 def cuda_time_ms(torch, fn, steps, flush=None):
@@ -1059,7 +1138,7 @@ def run_ours(args, rank, world, local_rank):
                        "cpu_baseline": gv_cpu,
                        "peak_gbs": hbm_peak, "peak_kind": hbm_kind,
                        "frac": gv_gbs / hbm_peak, "bytes_per_peak": 56},
-        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "clocks": clocks,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)

@@ -12,16 +12,17 @@ geometry parameters
     distance, y_center, z_center, tilt_x, tilt_y, tilt_z, wavelength, wedge,
     chi, t_x, t_y, t_z                       (ImageD11 parameter names)
 
-come from one forward and one reverse pass over the peaks, in FP64.  The small
-dense maps from those parameters to the detector matrix r = R(tilts).flip and
-the chi.wedge matrix M are written in torch so autograd chains through them.
+come from one forward and one reverse pass over the peaks, in FP64.  The
+parameters stay on the device: each kernel builds the detector matrix
+R3.R2.R1.flip and the chi.wedge matrix from them, and the backward pass
+contracts dL/d(matrices) with their derivatives itself, so no step reads the
+geometry on the host.
 
 :func:`refine_geometry` minimises the residuals over the geometry with the
 UBIs eliminated in closed form (each grain's least-squares UBI for the current
-g-vectors, an FP64 3x3 solve), using L-BFGS on the adjoint gradient.
+g-vectors, an FP64 3x3 solve in the same kernel), using L-BFGS on the adjoint
+gradient: one fused kernel and one reduction per evaluation.
 """
-import math
-
 import numpy as np
 
 from ._lib import lib, check
@@ -33,44 +34,13 @@ PARAMS = ("distance", "y_center", "z_center", "tilt_x", "tilt_y", "tilt_z", "wav
 SCALES = dict(distance=100.0, y_center=1.0, z_center=1.0, tilt_x=1e-3, tilt_y=1e-3,
               tilt_z=1e-3, wavelength=1e-5, wedge=1e-2, chi=1e-2, t_x=1.0, t_y=1.0, t_z=1.0)
 
+# fixed detector constants, in the order the kernels take them
+DETECTOR = ("y_size", "z_size", "omegasign", "o11", "o12", "o21", "o22")
+
 
 def _torch():
     import torch
     return torch
-
-
-def detector_matrix(tilt_x, tilt_y, tilt_z, flip):
-    """R3(tilt_x).R2(tilt_y).R1(tilt_z).flip (ImageD11/transform.py:51-82,
-    :688-692), differentiable in the tilts (radians)."""
-    torch = _torch()
-    z = torch.zeros((), dtype=torch.float64, device=tilt_x.device)
-    o = torch.ones((), dtype=torch.float64, device=tilt_x.device)
-    cz, sz = torch.cos(tilt_z), torch.sin(tilt_z)
-    cy, sy = torch.cos(tilt_y), torch.sin(tilt_y)
-    cx, sx = torch.cos(tilt_x), torch.sin(tilt_x)
-    r1 = torch.stack([torch.stack([cz, -sz, z]), torch.stack([sz, cz, z]),
-                      torch.stack([z, z, o])])
-    r2 = torch.stack([torch.stack([cy, z, sy]), torch.stack([z, o, z]),
-                      torch.stack([-sy, z, cy])])
-    r3 = torch.stack([torch.stack([o, z, z]), torch.stack([z, cx, -sx]),
-                      torch.stack([z, sx, cx])])
-    return r3 @ r2 @ r1 @ flip
-
-
-def wedgechi_matrix(wedge, chi):
-    """The chi.wedge matrix M of src/cdiffraction.c:117-142, wedge and chi in
-    degrees, differentiable."""
-    torch = _torch()
-    z = torch.zeros((), dtype=torch.float64, device=wedge.device)
-    o = torch.ones((), dtype=torch.float64, device=wedge.device)
-    w = wedge * (math.pi / 180.0)
-    c = chi * (math.pi / 180.0)
-    sw, cw, sc, cc = torch.sin(w), torch.cos(w), torch.sin(c), torch.cos(c)
-    W = torch.stack([torch.stack([cw, z, -sw]), torch.stack([z, o, z]),
-                     torch.stack([sw, z, cw])])
-    C = torch.stack([torch.stack([o, z, z]), torch.stack([z, cc, -sc]),
-                     torch.stack([z, sc, cc])])
-    return W @ C
 
 
 class PeakTable:
@@ -102,88 +72,115 @@ class PeakTable:
         self.y_size = float(geo["y_size"])
         self.z_size = float(geo["z_size"])
         self.omegasign = float(geo["omegasign"])
-        self.flip = torch.tensor([[1.0, 0.0, 0.0], [0.0, geo["o22"], geo["o21"]],
-                                  [0.0, geo["o12"], geo["o11"]]], dtype=torch.float64,
-                                 device=dev)
+        # host copy of the fixed constants, read by each call
+        self.det = np.array([float(geo[k]) for k in DETECTOR], dtype=np.float64)
         self.ws = torch.empty(lib.id11b_adjoint_workspace_bytes(max(self.ngrains, 1)) // 8,
                               dtype=torch.float64, device=dev)
 
-
-def _geom_host(r, M, t, lam, dist, yc, zc, peaks):
-    g = np.empty(28)
-    g[0:9] = r.detach().cpu().numpy().ravel()
-    g[9:18] = M.detach().cpu().numpy().ravel()
-    g[18:21] = t.detach().cpu().numpy()
-    g[21] = float(lam)
-    g[22] = float(dist)
-    g[23] = float(yc)
-    g[24] = float(zc)
-    g[25] = peaks.y_size
-    g[26] = peaks.z_size
-    g[27] = peaks.omegasign
-    return g
+    def _ptrs(self):
+        return (self.det.ctypes.data, self.sc.data_ptr(), self.fc.data_ptr(),
+                self.omega.data_ptr(), self.hkl.data_ptr(), self.offsets.data_ptr())
 
 
 def _stream():
     return _torch().cuda.current_stream().cuda_stream
 
 
+def _params(p):
+    torch = _torch()
+    p = p.detach()
+    if p.dtype != torch.float64 or not p.is_cuda or p.numel() != len(PARAMS):
+        raise ValueError("params: (12,) float64 CUDA tensor in the order of PARAMS")
+    return p.contiguous()
+
+
 class _Residuals(_torch().autograd.Function):
-    """res (n,3) = UBI_G . g(r, M, t, wavelength, distance, centres) - hkl."""
+    """res (n,3) = UBI_G . g(params) - hkl."""
 
     @staticmethod
-    def forward(ctx, r, M, t, lam, dist, yc, zc, ubis, peaks):
+    def forward(ctx, params, ubis, peaks):
         torch = _torch()
-        geom = _geom_host(r, M, t, lam, dist, yc, zc, peaks)
+        p = _params(params)
         u = ubis.detach().reshape(-1, 9).contiguous()
         res = torch.empty((peaks.n, 3), dtype=torch.float64, device=u.device)
-        ssq = torch.empty(max(peaks.ngrains, 1), dtype=torch.float64, device=u.device)
-        check(lib.id11b_dev_residuals(geom.ctypes.data, peaks.sc.data_ptr(), peaks.fc.data_ptr(),
-                                      peaks.omega.data_ptr(), peaks.hkl.data_ptr(),
-                                      peaks.offsets.data_ptr(), u.data_ptr(), peaks.ngrains,
-                                      res.data_ptr(), None, ssq.data_ptr(), _stream()),
-              "residuals")
+        check(lib.id11b_dev_residuals(p.data_ptr(), *peaks._ptrs(), u.data_ptr(), peaks.ngrains,
+                                      res.data_ptr(), None, None, _stream()), "residuals")
         ctx.peaks = peaks
-        ctx.geom = geom
-        ctx.save_for_backward(r, u)
+        ctx.save_for_backward(p, u)
         ctx.ubi_shape = ubis.shape
         return res
 
     @staticmethod
     def backward(ctx, grad_res):
         torch = _torch()
-        r, u = ctx.saved_tensors
+        p, u = ctx.saved_tensors
         peaks = ctx.peaks
         gr = grad_res.detach().to(torch.float64).contiguous()
         gu = torch.empty_like(u)
-        gl = torch.empty(22, dtype=torch.float64, device=u.device)
+        gp = torch.empty(len(PARAMS), dtype=torch.float64, device=u.device)
         check(lib.id11b_dev_residuals_adjoint(
-            ctx.geom.ctypes.data, peaks.sc.data_ptr(), peaks.fc.data_ptr(),
-            peaks.omega.data_ptr(), peaks.hkl.data_ptr(), peaks.offsets.data_ptr(),
-            u.data_ptr(), peaks.ngrains, gr.data_ptr(), gu.data_ptr(), gl.data_ptr(),
-            peaks.ws.data_ptr(), peaks.ws.numel() * 8, _stream()), "residuals_adjoint")
-        dM = gl[0:9].view(3, 3)
-        dlam = gl[9]
-        dt = gl[10:13]
-        A = gl[13:16]
-        dr = torch.zeros((3, 3), dtype=torch.float64, device=u.device)
-        dr[:, 1] = gl[16:19]
-        dr[:, 2] = gl[19:22]
-        ddist = A[0]
-        dyc = -peaks.y_size * torch.dot(r.detach()[:, 1], A)
-        dzc = -peaks.z_size * torch.dot(r.detach()[:, 2], A)
-        return dr, dM, dt, dlam, ddist, dyc, dzc, gu.view(ctx.ubi_shape), None
+            p.data_ptr(), *peaks._ptrs(), u.data_ptr(), peaks.ngrains, gr.data_ptr(),
+            gu.data_ptr(), gp.data_ptr(), peaks.ws.data_ptr(), peaks.ws.numel() * 8,
+            _stream()), "residuals_adjoint")
+        return gp, gu.view(ctx.ubi_shape), None
+
+
+class _Loss(_torch().autograd.Function):
+    """0.5 * sum |res|^2, with its gradients from the same fused pass."""
+
+    @staticmethod
+    def forward(ctx, params, ubis, peaks):
+        torch = _torch()
+        p = _params(params)
+        u = ubis.detach().reshape(-1, 9).contiguous()
+        L = torch.empty((), dtype=torch.float64, device=u.device)
+        gp = torch.empty(len(PARAMS), dtype=torch.float64, device=u.device)
+        gu = torch.empty_like(u) if ctx.needs_input_grad[1] else None
+        check(lib.id11b_dev_residual_loss(
+            p.data_ptr(), *peaks._ptrs(), u.data_ptr(), peaks.ngrains, L.data_ptr(),
+            gu.data_ptr() if gu is not None else None, gp.data_ptr(), None,
+            peaks.ws.data_ptr(), peaks.ws.numel() * 8, _stream()), "residual_loss")
+        ctx.save_for_backward(gp, gu if gu is not None else u)
+        ctx.has_gu = gu is not None
+        ctx.ubi_shape = ubis.shape
+        return L
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        gp, gu = ctx.saved_tensors
+        return (grad_out * gp, (grad_out * gu).view(ctx.ubi_shape) if ctx.has_gu else None,
+                None)
+
+
+class _ProjectedLoss(_torch().autograd.Function):
+    """min over every grain's UBI of 0.5 * sum |res|^2 (variable projection):
+    the loss at each grain's least-squares UBI, and its gradient with respect
+    to the geometry, from one fused kernel."""
+
+    @staticmethod
+    def forward(ctx, params, peaks, ubis_out):
+        torch = _torch()
+        p = _params(params)
+        L = torch.empty((), dtype=torch.float64, device=p.device)
+        gp = torch.empty(len(PARAMS), dtype=torch.float64, device=p.device)
+        check(lib.id11b_dev_residual_loss(
+            p.data_ptr(), *peaks._ptrs(), None, peaks.ngrains, L.data_ptr(), None,
+            gp.data_ptr(), ubis_out.data_ptr() if ubis_out is not None else None,
+            peaks.ws.data_ptr(), peaks.ws.numel() * 8, _stream()), "projected_loss")
+        ctx.save_for_backward(gp)
+        return L
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        gp, = ctx.saved_tensors
+        return grad_out * gp, None, None
 
 
 def residuals(params, ubis, peaks):
     """Residuals (n,3) of every assigned peak, differentiable with respect to
     ``params`` -- a (12,) float64 CUDA tensor in the order of PARAMS -- and
     ``ubis`` -- (ngrains,3,3) float64 CUDA tensor."""
-    dist, yc, zc, tx, ty, tz, lam, wedge, chi, t0, t1, t2 = params.unbind(0)
-    r = detector_matrix(tx, ty, tz, peaks.flip)
-    M = wedgechi_matrix(wedge, chi)
-    t = _torch().stack([t0, t1, t2])
-    return _Residuals.apply(r, M, t, lam, dist, yc, zc, ubis, peaks)
+    return _Residuals.apply(params, ubis, peaks)
 
 
 def params_tensor(geo):
@@ -195,46 +192,88 @@ def params_tensor(geo):
 def gvectors(params, peaks):
     """g-vectors (n,3) of the peaks for the geometry ``params`` (no gradient)."""
     torch = _torch()
-    with torch.no_grad():
-        dist, yc, zc, tx, ty, tz, lam, wedge, chi, t0, t1, t2 = params.detach().unbind(0)
-        r = detector_matrix(tx, ty, tz, peaks.flip)
-        M = wedgechi_matrix(wedge, chi)
-        t = torch.stack([t0, t1, t2])
-        geom = _geom_host(r, M, t, lam, dist, yc, zc, peaks)
-        dev = peaks.sc.device
-        zero = torch.zeros((max(peaks.ngrains, 1), 9), dtype=torch.float64, device=dev)
-        res = torch.empty((peaks.n, 3), dtype=torch.float64, device=dev)
-        g = torch.empty((peaks.n, 3), dtype=torch.float64, device=dev)
-        ssq = torch.empty(max(peaks.ngrains, 1), dtype=torch.float64, device=dev)
-        check(lib.id11b_dev_residuals(geom.ctypes.data, peaks.sc.data_ptr(), peaks.fc.data_ptr(),
-                                      peaks.omega.data_ptr(), peaks.hkl.data_ptr(),
-                                      peaks.offsets.data_ptr(), zero.data_ptr(), peaks.ngrains,
-                                      res.data_ptr(), g.data_ptr(), ssq.data_ptr(), _stream()),
-              "gvectors")
+    p = _params(params)
+    g = torch.empty((peaks.n, 3), dtype=torch.float64, device=p.device)
+    check(lib.id11b_dev_residuals(p.data_ptr(), *peaks._ptrs(), None, peaks.ngrains, None,
+                                  g.data_ptr(), None, _stream()), "gvectors")
     return g
 
 
-def best_ubis(g, peaks):
-    """Each grain's UBI minimising sum |UBI.g - h|^2 over its peaks:
-    UBI = (sum h g^T)(sum g g^T)^-1, an FP64 3x3 solve per grain."""
+def best_ubis(params, peaks):
+    """Each grain's UBI minimising sum |UBI.g - h|^2 over its peaks for the
+    g-vectors at ``params``: UBI = (sum h g^T)(sum g g^T)^-1, an FP64 3x3
+    solve per grain (UBI 0 where the normal matrix B = sum g g^T is singular,
+    det B <= 1e-10 trace(B)^3, as for fewer than three independent g)."""
     torch = _torch()
-    sizes = peaks.offsets[1:] - peaks.offsets[:-1]
-    gi = torch.repeat_interleave(torch.arange(peaks.ngrains, device=g.device), sizes)
-    h = peaks.hkl
-    A = torch.zeros((peaks.ngrains, 3, 3), dtype=torch.float64, device=g.device)
-    B = torch.zeros_like(A)
-    A.index_add_(0, gi, h[:, :, None] * g[:, None, :])
-    B.index_add_(0, gi, g[:, :, None] * g[:, None, :])
-    return torch.linalg.solve(B, A.transpose(1, 2)).transpose(1, 2).contiguous()
+    p = _params(params)
+    u = torch.empty((max(peaks.ngrains, 0), 3, 3), dtype=torch.float64, device=p.device)
+    check(lib.id11b_dev_best_ubis(p.data_ptr(), *peaks._ptrs(), peaks.ngrains, u.data_ptr(),
+                                  _stream()), "best_ubis")
+    return u
 
 
 def loss(params, ubis, peaks):
-    """0.5 * sum of squared residuals (differentiable)."""
-    r = residuals(params, ubis, peaks)
-    return 0.5 * (r * r).sum()
+    """0.5 * sum of squared residuals (differentiable in params and ubis)."""
+    return _Loss.apply(params, ubis, peaks)
 
 
-def refine_geometry(peaks, params0, free=None, max_iter=60, history=20):
+def projected_loss(params, peaks, ubis_out=None):
+    """0.5 * sum of squared residuals at every grain's least-squares UBI
+    (differentiable in params); the UBIs go to ``ubis_out`` ((ngrains,3,3)
+    float64 CUDA tensor) when given."""
+    return _ProjectedLoss.apply(params, peaks, ubis_out)
+
+
+class _BraggTheta(_torch().autograd.Function):
+    @staticmethod
+    def forward(ctx, ubs, peaks, wavelength):
+        torch = _torch()
+        b = ubs.detach().reshape(-1, 9).contiguous()
+        theta = torch.empty(peaks.n, dtype=torch.float64, device=b.device)
+        check(lib.id11b_dev_bragg_theta(b.data_ptr(), peaks.hkl.data_ptr(),
+                                        peaks.offsets.data_ptr(), peaks.ngrains,
+                                        float(wavelength), theta.data_ptr(), None, _stream()),
+              "bragg_theta")
+        ctx.save_for_backward(b)
+        ctx.peaks, ctx.wavelength, ctx.shape = peaks, float(wavelength), ubs.shape
+        return theta
+
+    @staticmethod
+    def backward(ctx, grad_theta):
+        torch = _torch()
+        b, = ctx.saved_tensors
+        peaks = ctx.peaks
+        gt = grad_theta.detach().to(torch.float64).contiguous()
+        gb = torch.empty_like(b)
+        check(lib.id11b_dev_bragg_theta_adjoint(b.data_ptr(), peaks.hkl.data_ptr(),
+                                                peaks.offsets.data_ptr(), peaks.ngrains,
+                                                ctx.wavelength, gt.data_ptr(), gb.data_ptr(),
+                                                _stream()), "bragg_theta_adjoint")
+        return gb.view(ctx.shape), None, None
+
+
+def bragg_theta(ubs, peaks, wavelength):
+    """Bragg angle theta (degrees, (n,)) of every assigned reflection computed
+    from its grain's UB matrix -- ``ubs`` (ngrains,3,3) float64 CUDA tensor,
+    the inverse of the UBI -- as ImageD11 src/deriv.c:38-53 computes it
+    (asin(wavelength |UB h| / 2)); differentiable in ``ubs``."""
+    return _BraggTheta.apply(ubs, peaks, wavelength)
+
+
+def bragg_theta_jacobian(ubs, peaks, wavelength):
+    """(theta (n,), dtheta/dUB (n,3,3)) per reflection, forward mode, the
+    pair ImageD11 src/deriv.c:38-53 returns in tth_calc[0] and tth_calc[1:10]."""
+    torch = _torch()
+    b = ubs.detach().reshape(-1, 9).contiguous()
+    theta = torch.empty(peaks.n, dtype=torch.float64, device=b.device)
+    jac = torch.empty((peaks.n, 3, 3), dtype=torch.float64, device=b.device)
+    check(lib.id11b_dev_bragg_theta(b.data_ptr(), peaks.hkl.data_ptr(), peaks.offsets.data_ptr(),
+                                    peaks.ngrains, float(wavelength), theta.data_ptr(),
+                                    jac.data_ptr(), _stream()), "bragg_theta")
+    return theta, jac
+
+
+def refine_geometry(peaks, params0, free=None, max_iter=60, history=20, max_eval=None):
     """Refine the geometry by L-BFGS with every grain's UBI re-solved in closed
     form at each evaluation (variable projection: at the best UBIs the loss
     gradient with respect to the geometry is the partial derivative, which the
@@ -246,12 +285,15 @@ def refine_geometry(peaks, params0, free=None, max_iter=60, history=20):
     against chi (both rotate about the beam); the optimiser then settles
     anywhere along them, which leaves the residuals, the other parameters and
     the combinations z_center*z_size + t_z and tilt_x - chi (radians) fixed.
-    Returns (params, ubis, history of loss values)."""
+    ``max_eval``: evaluation budget (default max_iter * 5 // 4 + 20, so that
+    the line search of even one iteration can bracket its step).
+    Returns (params, ubis, history of loss values); the last history entry is
+    the loss at the returned params."""
     torch = _torch()
     free = [p for p in PARAMS if p != "wavelength"] if free is None else list(free)
     mask = torch.tensor([p in free for p in PARAMS], dtype=torch.float64, device="cuda")
     scale = torch.tensor([SCALES[p] for p in PARAMS], dtype=torch.float64, device="cuda")
-    base = params0.detach().to(torch.float64).clone()
+    base = _params(params0).clone()
     x = torch.zeros(len(PARAMS), dtype=torch.float64, device="cuda", requires_grad=True)
     hist = []
 
@@ -260,16 +302,19 @@ def refine_geometry(peaks, params0, free=None, max_iter=60, history=20):
 
     def closure():
         opt.zero_grad()
-        p = current()
-        u = best_ubis(gvectors(p, peaks), peaks)
-        value = loss(p, u, peaks)
+        value = projected_loss(current(), peaks)
         value.backward()
         hist.append(float(value.detach()))
         return value
 
-    opt = torch.optim.LBFGS([x], lr=1.0, max_iter=max_iter, history_size=history,
-                            tolerance_grad=1e-14, tolerance_change=1e-16,
-                            line_search_fn="strong_wolfe")
+    if max_eval is None:
+        max_eval = max_iter * 5 // 4 + 20
+    opt = torch.optim.LBFGS([x], lr=1.0, max_iter=max_iter, max_eval=max_eval,
+                            history_size=history, tolerance_grad=1e-14,
+                            tolerance_change=1e-16, line_search_fn="strong_wolfe")
     opt.step(closure)
     p = current().detach()
-    return p, best_ubis(gvectors(p, peaks), peaks), hist
+    u = torch.empty((peaks.ngrains, 3, 3), dtype=torch.float64, device="cuda")
+    with torch.no_grad():
+        hist.append(float(projected_loss(p, peaks, u)))
+    return p, u, hist

@@ -92,6 +92,24 @@ int finish(Staging& s) {
     return s.status;
 }
 
+// Small results come back through one pinned buffer per host thread (a copy
+// from device to pageable memory costs a staging step per call).
+struct LsqResult {
+    double u[9];
+    double mean;
+    int32_t n;
+    int32_t pad;
+};
+
+LsqResult* pinned_result() {
+    static thread_local LsqResult* r = nullptr;
+    if (!r && cudaMallocHost((void**)&r, sizeof(LsqResult)) != cudaSuccess) {
+        cudaGetLastError();
+        r = nullptr;
+    }
+    return r;
+}
+
 }  // namespace
 
 extern "C" void id11b_compute_gv(double xlylzl[][3], double omega[], double omegasign,
@@ -158,33 +176,31 @@ static void lsq_host(int mode, double ubi[3][3], double gv[][3], double tol, int
                      int label, int* n_out, double* mean_out, int ng) {
     if (ng < 0) { t_last_status = ID11B_ERR_ARG; return; }
     int64_t wsb = id11b_lsq_workspace_bytes(ng);
-    Staging s(sizeof(double) * (3 * (size_t)ng + 9) + sizeof(int) * (size_t)(mode ? ng : 0) +
-              (size_t)wsb + 64);
-    double* du = s.take<double>(9);
+    Staging s(sizeof(double) * 3 * (size_t)ng + sizeof(LsqResult) +
+              sizeof(int) * (size_t)(mode ? ng : 0) + (size_t)wsb + 64);
+    LsqResult* dr = s.take<LsqResult>(1);  // UBI, then n and mean next to it
     double* dg = s.take<double>(3 * (size_t)ng);
     int32_t* dl = mode ? s.take<int32_t>(ng) : nullptr;
     char* ws = s.take<char>(wsb);
-    int32_t* dn = s.take<int32_t>(1);
-    double* dm = s.take<double>(1);
-    s.h2d(du, ubi, sizeof(double) * 9);
+    s.h2d(dr->u, ubi, sizeof(double) * 9);
     s.h2d(dg, gv, sizeof(double) * 3 * (size_t)ng);
     if (mode) s.h2d(dl, labels, sizeof(int32_t) * (size_t)ng);
     if (!s.status) {
         if (mode == 0)
-            s.run(id11b_dev_score_and_refine(du, dg, tol, ng, dn, dm, ws, wsb, s.st));
+            s.run(id11b_dev_score_and_refine(dr->u, dg, tol, ng, &dr->n, &dr->mean, ws, wsb,
+                                             s.st));
         else
-            s.run(id11b_dev_refine_assigned(du, dg, dl, label, ng, dn, dm, ws, wsb, s.st));
+            s.run(id11b_dev_refine_assigned(dr->u, dg, dl, label, ng, &dr->n, &dr->mean, ws, wsb,
+                                            s.st));
     }
-    int32_t n = 0;
-    double mean = 0.;
-    double u[9];
-    s.d2h(u, du, sizeof(u));
-    s.d2h(&n, dn, sizeof(n));
-    s.d2h(&mean, dm, sizeof(mean));
+    LsqResult local;
+    LsqResult* hr = pinned_result();
+    if (!hr) hr = &local;
+    s.d2h(hr, dr, sizeof(LsqResult));
     if (finish(s) == ID11B_OK) {
-        memcpy(ubi, u, sizeof(u));
-        *n_out = n;
-        *mean_out = mean;
+        memcpy(ubi, hr->u, sizeof(hr->u));
+        *n_out = hr->n;
+        *mean_out = hr->mean;
     }
 }
 

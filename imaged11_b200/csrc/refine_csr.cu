@@ -62,12 +62,24 @@ struct RefineSmem {
 __constant__ int c_hrow[6] = {0, 0, 0, 1, 1, 2};
 __constant__ int c_hcol[6] = {0, 1, 2, 1, 2, 2};
 
-template <int NT>
+// Compensated FP32 accumulation (the F32C variant): a sum kept as s + c with
+// every addition's rounding error recovered exactly (TwoSum) and every
+// product's by an FMA (TwoProduct), Ogita, Rump and Oishi, "Accurate sum and
+// dot product", SIAM J. Sci. Comput. 26 (2005) -- as accurate as a sum in
+// twice the working precision.
+__device__ __forceinline__ void comp_add(float& s, float& c, float x) {
+    const float t = s + x;
+    const float bp = t - s;
+    c += (s - (t - bp)) + (x - bp);
+    s = t;
+}
+
+template <int NT, bool F32C = false>
 __global__ void __launch_bounds__(NT)
 k_refine_csr(double* __restrict__ ubis, const double* __restrict__ gv,
              const int64_t* __restrict__ off, const int* __restrict__ order, int ngrains,
              double tolsq, int iters, int* __restrict__ queue, int* __restrict__ npk,
-             double* __restrict__ mean) {
+             double* __restrict__ mean, double gmax) {
     __shared__ RefineSmem<NT> sm;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     for (int slot = blockIdx.x;; slot += gridDim.x) {
@@ -88,6 +100,28 @@ k_refine_csr(double* __restrict__ ubis, const double* __restrict__ gv,
             double acc[17];
 #pragma unroll
             for (int f = 0; f < 17; f++) acc[f] = 0.;
+            // F32C: screening thresholds of the proven band (score_batch.cu) for
+            // this UBI, FP32 copy of the UBI, compensated R and drlv2 sums,
+            // exact integer H
+            float lo32 = 0.f, hi32 = 0.f, u32[9], rs[9], rc[9], ss32 = 0.f, sc32 = 0.f;
+            int hint[6] = {0, 0, 0, 0, 0, 0}, nacc = 0;
+            if (F32C) {
+                double S = 0.;
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+                    S = fmax(S, fabs(u[3 * r]) + fabs(u[3 * r + 1]) + fabs(u[3 * r + 2]));
+                const double E = 6.0 * 5.9604644775390625e-08 * S * (1. + 1e-15) * gmax;
+                const double t = sqrt(tolsq);
+                const double band = 1.25 * (3.0 * E * (2.0 * (t + 1e-3) + E) +
+                                            4.0 * 5.9604644775390625e-08 * (tolsq + 0.01));
+                lo32 = __double2float_rd(tolsq - band);
+                hi32 = __double2float_ru(tolsq + band);
+#pragma unroll
+                for (int e = 0; e < 9; e++) {
+                    u32[e] = __double2float_rn(u[e]);
+                    rs[e] = rc[e] = 0.f;
+                }
+            }
             // kU peaks per lane per step: all their loads are issued before any
             // is used, so one memory latency covers kU peaks (the segment is
             // read-only and re-read every round, so later rounds hit L1)
@@ -106,6 +140,53 @@ k_refine_csr(double* __restrict__ ubis, const double* __restrict__ gv,
 #pragma unroll
                 for (int q = 0; q < kU; q++) {
                     if (kb + (int64_t)q * NT >= k1) break;
+                    if (F32C) {
+                        // g split exactly enough into hi + lo floats
+                        float gh[3], gl[3], ihf[3], t[3];
+#pragma unroll
+                        for (int i = 0; i < 3; i++) {
+                            gh[i] = __double2float_rn(gg[q][i]);
+                            gl[i] = __double2float_rn(gg[q][i] - (double)gh[i]);
+                        }
+                        const float M = 12582912.0f;  // 1.5 * 2^23
+#pragma unroll
+                        for (int r = 0; r < 3; r++) {
+                            const float h = fmaf(u32[3 * r + 2], gh[2],
+                                                 fmaf(u32[3 * r + 1], gh[1], u32[3 * r] * gh[0]));
+                            ihf[r] = __fsub_rn(__fadd_rn(h, M), M);
+                            t[r] = h - ihf[r];
+                        }
+                        float s32 = fmaf(t[2], t[2], fmaf(t[1], t[1], t[0] * t[0]));
+                        if (!(s32 < hi32)) continue;
+                        if (!(s32 < lo32)) {  // inside the band: the exact decision
+                            double ih[3];
+                            const double s = drlv2_exact(u, gg[q][0], gg[q][1], gg[q][2], ih);
+                            if (!(s < tolsq)) continue;
+#pragma unroll
+                            for (int r = 0; r < 3; r++) ihf[r] = (float)ih[r];
+                            s32 = (float)s;
+                        }
+#pragma unroll
+                        for (int i = 0; i < 3; i++)
+#pragma unroll
+                            for (int j = 0; j < 3; j++) {
+                                // ih_j * g_i = ih_j * gh_i (TwoProduct) + ih_j * gl_i
+                                const float p = ihf[j] * gh[i];
+                                const float pe = fmaf(ihf[j], gh[i], -p);
+                                comp_add(rs[3 * i + j], rc[3 * i + j], p);
+                                rc[3 * i + j] += pe + ihf[j] * gl[i];
+                            }
+                        const int a = (int)ihf[0], b = (int)ihf[1], c = (int)ihf[2];
+                        hint[0] += a * a;
+                        hint[1] += b * a;
+                        hint[2] += c * a;
+                        hint[3] += b * b;
+                        hint[4] += c * b;
+                        hint[5] += c * c;
+                        comp_add(ss32, sc32, s32);
+                        nacc++;
+                        continue;
+                    }
                     double ih[3];
                     const double s = drlv2_exact(u, gg[q][0], gg[q][1], gg[q][2], ih);
                     if (!(s < tolsq)) continue;
@@ -127,6 +208,14 @@ k_refine_csr(double* __restrict__ ubis, const double* __restrict__ gv,
                     acc[15] = dadd(acc[15], s);
                     acc[16] += 1.0;
                 }
+            }
+            if (F32C) {  // to FP64 for the fixed reduction: s + c, exact integers
+#pragma unroll
+                for (int e = 0; e < 9; e++) acc[e] = (double)rs[e] + (double)rc[e];
+#pragma unroll
+                for (int e = 0; e < 6; e++) acc[9 + e] = (double)hint[e];
+                acc[15] = (double)ss32 + (double)sc32;
+                acc[16] = (double)nacc;
             }
 #pragma unroll
             for (int f = 0; f < 17; f++) acc[f] = warp_sum(acc[f]);
@@ -200,22 +289,23 @@ static int sm_count_rc() {
 
 using namespace id11b;
 
-template <int NT>
+template <int NT, bool F32C = false>
 static int launch_refine(double* ubis, const double* gv, const int64_t* offsets,
                          const int32_t* order, int32_t ngrains, double tolsq, int iters,
-                         int* queue, int32_t* npk, double* mean, cudaStream_t st) {
+                         int* queue, int32_t* npk, double* mean, cudaStream_t st,
+                         double gmax = 0.) {
     int grid = ngrains;
     if (queue) {
         static int occ = 0;
         if (!occ) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_refine_csr<NT>, NT, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_refine_csr<NT, F32C>, NT, 0);
             if (occ < 1) occ = 1;
         }
         const int cap = sm_count_rc() * occ;
         grid = ngrains < cap ? ngrains : cap;
     }
-    k_refine_csr<NT><<<grid, NT, 0, st>>>(ubis, gv, offsets, order, ngrains, tolsq, iters,
-                                          queue, npk, mean);
+    k_refine_csr<NT, F32C><<<grid, NT, 0, st>>>(ubis, gv, offsets, order, ngrains, tolsq, iters,
+                                                queue, npk, mean, gmax);
     ID11B_CHECK_LAUNCH();
     return ID11B_OK;
 }
@@ -249,4 +339,27 @@ extern "C" int id11b_dev_refine_csr(double* ubis, const double* gv, const int64_
         case 512: return launch_refine<512>(ubis, gv, offsets, order, ngrains, tolsq, iters, queue, npk, mean_drlv2, st);
         default: return launch_refine<128>(ubis, gv, offsets, order, ngrains, tolsq, iters, queue, npk, mean_drlv2, st);
     }
+}
+
+// The same rounds with FP32 screening (the proven band, FP64 inside it) and
+// compensated FP32 normal-equation sums (integer H), FP64 3x3 solves: the
+// accumulation the batched design could use instead of FP64 sums.  gmax:
+// bound on every |g_j| of the segments (the band's input); g-vectors beyond
+// 1024 or non-finite are not supported by this variant (ID11B_ERR_ARG).
+extern "C" int id11b_dev_refine_csr_f32c(double* ubis, const double* gv, const int64_t* offsets,
+                                         const int32_t* order, int32_t ngrains, double tol,
+                                         int iters, double gmax, int32_t* npk,
+                                         double* mean_drlv2, void* workspace, int64_t ws_bytes,
+                                         void* stream) {
+    if (ngrains < 0 || iters < 0 || !(gmax >= 0.) || !(gmax <= 1024.) || !(tol >= 0.) ||
+        !(tol < 0.4))
+        return ID11B_ERR_ARG;
+    if (ngrains > 0 && (!ubis || !offsets)) return ID11B_ERR_ARG;
+    if (!workspace || ws_bytes < id11b_refine_csr_workspace_bytes()) return ID11B_ERR_ARG;
+    if (ngrains == 0 || iters == 0) return ID11B_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    int* queue = (int*)workspace;
+    ID11B_CHECK(cudaMemsetAsync(queue, 0, sizeof(int), st));
+    return launch_refine<64, true>(ubis, gv, offsets, order, ngrains, tol * tol, iters, queue,
+                                   npk, mean_drlv2, st, gmax);
 }

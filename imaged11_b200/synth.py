@@ -314,6 +314,31 @@ def simulate(ngrains, cell="Al", gmax=1.0, seed=0, geo=None, sigma_px=0.5, sigma
     return out
 
 
+def grain_gvectors(counts, cell, rng, sigma=5e-4):
+    """Per-grain g-vector sets without a detector: grain i (orientation uniform
+    on SO(3)) keeps its counts[i] shortest allowed reflections (a per-grain |g|
+    cutoff; hkl and -hkl both), g = U.B.hkl plus Gaussian noise of sigma
+    (1/A) per component.  Returns (gv (n,3) sorted by grain, offsets
+    (ngrains+1,) int64, true UBIs (ngrains,3,3))."""
+    counts = np.asarray(counts, dtype=np.int64)
+    a, b, c, al, be, ga, lat = CELLS[cell]
+    B = b_matrix(a, b, c, al, be, ga)
+    gmax = 0.5
+    while True:  # reflections enough for the largest grain
+        hkl, _ = hkl_list(cell, gmax)
+        if len(hkl) >= counts.max():
+            break
+        gmax *= 1.25
+    U = random_rotations(len(counts), rng)
+    UB = U @ B
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    gv = np.empty((int(offsets[-1]), 3))
+    for i, k in enumerate(counts):
+        gv[offsets[i]:offsets[i + 1]] = hkl[:k] @ UB[i].T
+    gv += rng.normal(size=gv.shape) * sigma
+    return gv, offsets, np.linalg.inv(UB)
+
+
 def trial_ubis(true_ubis, ntrial, frac_true, angle_deg, rng, cell="Al"):
     """Trial UBIs: frac_true of them perturbed copies of true UBIs, the rest
     uniformly random orientations of the same cell."""

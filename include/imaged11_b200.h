@@ -371,6 +371,19 @@ int id11b_dev_refine_csr(double *ubis, const double *gv, const int64_t *offsets,
                          int persistent, int threads, int32_t *npk, double *mean_drlv2,
                          void *workspace, int64_t ws_bytes, void *stream);
 
+/* Per-grain refinement as id11b_dev_refine_csr (persistent, 64-thread CTAs)
+ * with FP32 screening -- the proven error band of id11b_dev_score_batch, FP64
+ * inside it -- and compensated FP32 normal-equation sums (error-free products
+ * and TwoSum; H as exact integers), FP64 3x3 solves.  The same accepted pairs
+ * and peak counts; UBIs agree with the FP64 sums to ~1e-14 relative, mean
+ * drlv2 to the band (~1e-6 relative).  gmax: a bound on every |g_j| (<= 1024,
+ * finite g only); tol < 0.4.  No counterpart in the reference: its
+ * score_and_refine sums in FP64 (ImageD11 src/closest.c:267-345). */
+int id11b_dev_refine_csr_f32c(double *ubis, const double *gv, const int64_t *offsets,
+                              const int32_t *order, int32_t ngrains, double tol, int iters,
+                              double gmax, int32_t *npk, double *mean_drlv2, void *workspace,
+                              int64_t ws_bytes, void *stream);
+
 /* Per-grain translation refinement: minimises, for every grain G at once, the
  * objective of ImageD11/refinegrains.py refinepositions / gof (:517-560,
  * :639-660): the sum over grain G's peaks with drlv2 < tol^2 of
@@ -394,30 +407,68 @@ int id11b_dev_refine_translations(const double *xyz, const double *omega,
  * quantity refinegrains.gof minimises by Nelder-Mead, ImageD11/refinegrains.py
  * :517-560).  Peaks are stored grain by grain: grain G owns peaks
  * offsets[G] .. offsets[G+1]-1, with detector positions sc (slow), fc (fast),
- * omega (degrees) and assigned integer hkl (n,3 doubles).  geom_host holds 28
- * doubles: r (9, detector rotation . flip), M (9, chi.wedge), t (3),
- * wavelength, distance, y_center, z_center, y_size, z_size, omegasign.
+ * omega (degrees) and assigned integer hkl (n,3 doubles).
+ *
+ * params: 12 doubles in DEVICE memory -- distance, y_center, z_center,
+ * tilt_x, tilt_y, tilt_z (radians), wavelength, wedge, chi (degrees), t_x,
+ * t_y, t_z (ImageD11 parameter names); every launch builds the detector
+ * matrix R3(tilt_x).R2(tilt_y).R1(tilt_z).flip (ImageD11/transform.py:51-82)
+ * and chi.wedge from them on the device, so no call reads the geometry on
+ * the host.  detector: 7 HOST doubles, the fixed constants y_size, z_size,
+ * omegasign, o11, o12, o21, o22 (read during the call).
+ *
  * id11b_dev_residuals writes res (n,3) = UBI_G.g - hkl, optionally gvec (n,3),
- * and ssq (ngrains) = per-grain sum of squared residuals.
+ * and ssq (ngrains, optional) = per-grain sum of squared residuals; with
+ * ubis NULL it writes gvec only (hkl and res unused).
  * id11b_dev_residuals_adjoint takes grad_res = dL/dres (n,3) and writes
- * grad_ubis (ngrains,9) = dL/dUBI and grad_global (22) = dL/dM (9, row-major),
- * dL/dwavelength, dL/dt (3), sum of dL/dxyz (3), sum of dL/dxyz * v1 (3) and
- * sum of dL/dxyz * v2 (3) with v1 = (fc - y_center) y_size,
- * v2 = (sc - z_center) z_size -- the contractions with d(r, M)/d(tilts,
- * wedge, chi) and with the centres and distance are left to the caller.
+ * grad_ubis (ngrains,9, optional) = dL/dUBI and grad_params (12, device) =
+ * dL/dparams.
+ * id11b_dev_residual_loss writes loss (1, device) = 0.5 sum |res|^2 and its
+ * gradients in one pass over the peaks: at the given ubis (grad_ubis
+ * optional), or, with ubis NULL, at each grain's least-squares UBI for the
+ * current g-vectors (variable projection; the UBIs go to ubis_out when it is
+ * not NULL, grad_ubis must be NULL -- it is zero there).
+ * id11b_dev_best_ubis writes each grain's least-squares UBI
+ * (sum h g^T)(sum g g^T)^-1 for the g-vectors at params; a grain whose
+ * normal matrix B = sum g g^T is singular (det B <= 1e-10 trace(B)^3, as
+ * for fewer than three independent g) gets UBI 0.
  * FP64; reductions in a fixed order (deterministic).  Workspace:
  * id11b_adjoint_workspace_bytes(ngrains). */
 int64_t id11b_adjoint_workspace_bytes(int32_t ngrains);
-int id11b_dev_residuals(const double *geom_host, const double *sc, const double *fc,
-                        const double *omega, const double *hkl, const int64_t *offsets,
-                        const double *ubis, int32_t ngrains, double *res, double *gvec,
-                        double *ssq, void *stream);
-int id11b_dev_residuals_adjoint(const double *geom_host, const double *sc, const double *fc,
-                                const double *omega, const double *hkl,
-                                const int64_t *offsets, const double *ubis, int32_t ngrains,
-                                const double *grad_res, double *grad_ubis,
-                                double *grad_global, void *workspace, int64_t ws_bytes,
+int id11b_dev_residuals(const double *params, const double *detector, const double *sc,
+                        const double *fc, const double *omega, const double *hkl,
+                        const int64_t *offsets, const double *ubis, int32_t ngrains,
+                        double *res, double *gvec, double *ssq, void *stream);
+int id11b_dev_residuals_adjoint(const double *params, const double *detector,
+                                const double *sc, const double *fc, const double *omega,
+                                const double *hkl, const int64_t *offsets, const double *ubis,
+                                int32_t ngrains, const double *grad_res, double *grad_ubis,
+                                double *grad_params, void *workspace, int64_t ws_bytes,
                                 void *stream);
+int id11b_dev_residual_loss(const double *params, const double *detector, const double *sc,
+                            const double *fc, const double *omega, const double *hkl,
+                            const int64_t *offsets, const double *ubis, int32_t ngrains,
+                            double *loss, double *grad_ubis, double *grad_params,
+                            double *ubis_out, void *workspace, int64_t ws_bytes, void *stream);
+int id11b_dev_best_ubis(const double *params, const double *detector, const double *sc,
+                        const double *fc, const double *omega, const double *hkl,
+                        const int64_t *offsets, int32_t ngrains, double *ubis_out,
+                        void *stream);
+
+/* Bragg angle of each assigned reflection computed from its grain's UB
+ * matrix (ubs: ngrains x 9, row-major; hkl, offsets as above), in degrees,
+ * and its derivative with respect to UB, the quantities ImageD11
+ * src/deriv.c:38-53 (g_to_k) computes: g = UB h, t = wavelength |g| / 2,
+ * theta = asin(t), dtheta/dUB_ij = (180/pi) wavelength g_i h_j /
+ * (2 |g| sqrt(1 - t^2)).  dtheta_dub (n,9) is optional.  The adjoint takes
+ * grad_theta (n) and writes grad_ubs (ngrains,9) = sum over each grain's
+ * peaks of grad_theta dtheta/dUB (fixed order).  FP64. */
+int id11b_dev_bragg_theta(const double *ubs, const double *hkl, const int64_t *offsets,
+                          int32_t ngrains, double wavelength, double *theta,
+                          double *dtheta_dub, void *stream);
+int id11b_dev_bragg_theta_adjoint(const double *ubs, const double *hkl,
+                                  const int64_t *offsets, int32_t ngrains, double wavelength,
+                                  const double *grad_theta, double *grad_ubs, void *stream);
 
 /* Synchronising read of the last batch call's statistics from its workspace:
  * FP64 re-evaluations, UBIs routed wholly to FP64, and the device error flag

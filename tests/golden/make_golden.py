@@ -17,6 +17,11 @@ Outputs come from two reference implementations:
   with stub ``fabio``/``cImageD11`` modules because only its numpy functions
   are used.
 
+The derivatives fixture holds the reference's own hand-derived derivatives:
+dg/dt of ImageD11/sandbox/fittrans2.py (d_XSXB_to_gv, its function
+definitions run from the file) and theta, dtheta/dUB of src/deriv.c (g_to_k,
+compiled by ``make -C oracle deriv`` with its main renamed).
+
 The adjoint fixture holds the reference forward model's loss and its central
 finite-difference gradients (compute_xyz_lab -> compute_tth_eta_from_xyz ->
 compute_g_vectors -> UBI.g - h) with respect to the 12 geometry parameters
@@ -292,6 +297,106 @@ def cases_adjoint(tr):
                 adj_truth=np.array([truth[k] for k in ADJ_PARAMS]))
 
 
+def load_fittrans2(ref_root):
+    """k_to_g and d_XSXB_to_gv from the reference's ImageD11/sandbox/fittrans2.py
+    (its module-level imports need matplotlib and numba, so only these
+    function definitions are taken from the file and run)."""
+    import ast
+    path = os.path.join(ref_root, "ImageD11", "sandbox", "fittrans2.py")
+    tree = ast.parse(open(path).read())
+    fns = [n for n in tree.body
+           if isinstance(n, ast.FunctionDef) and n.name in ("k_to_g", "d_XSXB_to_gv")]
+    ns = {"np": np}
+    exec(compile(ast.Module(body=fns, type_ignores=[]), path, "exec"), ns)
+    return ns["k_to_g"], ns["d_XSXB_to_gv"]
+
+
+def load_deriv(ref_root):
+    """g_to_k and make_ax of the reference's src/deriv.c, compiled by
+    ``make -C oracle deriv`` into oracle/_ref/libderiv_ref.so."""
+    import ctypes
+    so = os.path.join(REPO, "oracle", "_ref", "libderiv_ref.so")
+    if not os.path.exists(so):
+        import subprocess
+        subprocess.check_call(["make", "-C", os.path.join(REPO, "oracle"), "deriv",
+                               "REF=" + ref_root])
+    lib = ctypes.CDLL(so)
+    p = ctypes.POINTER(ctypes.c_double)
+    lib.g_to_k.argtypes = [p, p, p, p, ctypes.c_double, p, p, p, p, p]
+    lib.g_to_k.restype = ctypes.c_int
+    lib.make_ax.argtypes = [p, p, p, p]
+    lib.make_ax.restype = ctypes.c_int
+    return lib
+
+
+def cases_derivatives(tr, ref_root):
+    """Hand-derived derivatives of the reference, for the adjoint tests:
+
+    * dg/dt (the grain translation) of ImageD11/sandbox/fittrans2.py:39-77
+      (d_XSXB_to_gv) on peaks computed through the reference's
+      compute_xyz_lab and k_to_g with wedge and chi set;
+    * theta and dtheta/dUB of src/deriv.c:38-53 (g_to_k's tth_calc[0:10])
+      for the UB matrices and hkl of simulated grains."""
+    import ctypes
+    k_to_g, d_xsxb = load_fittrans2(ref_root)
+    gvg = sys.modules["ImageD11.gv_general"]
+    truth = synth.default_geometry(distance=152300., y_center=1024 + 3.7, z_center=1024 - 2.1,
+                                   tilt_x=0.004, tilt_y=-0.002, tilt_z=0.006, wedge=0.3,
+                                   chi=-0.2, t_x=5., t_y=-3., t_z=2.)
+    ps = synth.simulate(3, "Al", gmax=1.2, seed=23, geo=truth, sigma_px=0.3, sigma_om=0.02,
+                        noise_frac=0.0, translation=(5., -3., 2.))
+    idx, off = ps.grain_offsets()
+    s, f, om, hkl = ps.s[idx], ps.f[idx], ps.omega[idx], ps.hkl[idx]
+    pars = dict(truth, t_x=4.0, t_y=-2.5, t_z=1.5)
+    xyz = tr.compute_xyz_lab((s, f), **pars)
+    omr = np.radians(om * pars["omegasign"])
+    cw = gvg.chiwedge(pars["chi"], pars["wedge"])
+    XS = k_to_g(xyz, np.cos(omr), np.sin(omr), cw)
+    beam = np.zeros((3, len(om)))
+    beam[0] = 1.0
+    XB = k_to_g(beam, np.cos(omr), np.sin(omr), cw)
+    g, dgdt = d_xsxb(XS, XB, pars["t_x"], pars["t_y"], pars["t_z"], pars["wavelength"])
+    # the same g through the reference transform (a check of the frames)
+    tth, eta = tr.compute_tth_eta_from_xyz(xyz, om * pars["omegasign"], t_x=pars["t_x"],
+                                           t_y=pars["t_y"], t_z=pars["t_z"],
+                                           wedge=pars["wedge"], chi=pars["chi"])
+    gref = tr.compute_g_vectors(tth, eta, om * pars["omegasign"], pars["wavelength"],
+                                wedge=pars["wedge"], chi=pars["chi"])
+    assert np.abs(g - gref).max() < 1e-12
+    # deriv.c: UB = inv(UBI) of each grain, reflections of its peaks
+    lib = load_deriv(ref_root)
+    D = ctypes.POINTER(ctypes.c_double)
+
+    def arr(a):
+        return np.ascontiguousarray(a, dtype=np.float64)
+
+    eye = arr(np.eye(3).ravel())
+    axis, bm, ax = arr([0., 0., 1.]), arr([1., 0., 0.]), np.zeros(19)
+    lib.make_ax(eye.ctypes.data_as(D), axis.ctypes.data_as(D), bm.ctypes.data_as(D),
+                ax.ctypes.data_as(D))
+    ubs = np.array([np.linalg.inv(u) for u in ps.ubis])
+    grain = np.repeat(np.arange(len(off) - 1), np.diff(off))
+    theta = np.empty(len(hkl))
+    dtheta = np.empty((len(hkl), 9))
+    for k in range(len(hkl)):
+        h4 = arr([hkl[k, 0], hkl[k, 1], hkl[k, 2], 1.0])
+        ub = arr(ubs[grain[k]].ravel())
+        gc, kc = np.zeros(3), np.zeros(3)
+        tc, ec, oc = np.zeros(10), np.zeros(10), np.zeros(10)
+        lib.g_to_k(h4.ctypes.data_as(D), ub.ctypes.data_as(D), ax.ctypes.data_as(D),
+                   eye.ctypes.data_as(D), pars["wavelength"], gc.ctypes.data_as(D),
+                   kc.ctypes.data_as(D), tc.ctypes.data_as(D), ec.ctypes.data_as(D),
+                   oc.ctypes.data_as(D))
+        theta[k] = tc[0]
+        dtheta[k] = tc[1:10]
+    return dict(der_s=s, der_f=f, der_omega=om, der_hkl=hkl, der_offsets=off,
+                der_params=np.array([pars[k] for k in ADJ_PARAMS]),
+                der_const=np.array([pars["y_size"], pars["z_size"], pars["omegasign"],
+                                    pars["o11"], pars["o12"], pars["o21"], pars["o22"]]),
+                der_g=g.T.copy(), der_dgdt=np.moveaxis(dgdt, 2, 0).copy(),
+                der_ubs=ubs, der_theta=theta, der_dtheta=dtheta)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("IMAGED11_REF")
     if not ref_root:
@@ -303,6 +408,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "compute_xlylzl.npz"), **cases_xlylzl(ref, tr))
     np.savez_compressed(os.path.join(HERE, "scoring.npz"), **cases_scoring(ref))
     np.savez_compressed(os.path.join(HERE, "adjoint.npz"), **cases_adjoint(tr))
+    np.savez_compressed(os.path.join(HERE, "derivatives.npz"), **cases_derivatives(tr, ref_root))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

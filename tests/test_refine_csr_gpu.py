@@ -69,3 +69,23 @@ def test_refine_csr_deterministic(grains, cuda):
     a = batch.GrainSet(gv, off, u0).refine(0.05, 3)[0].cpu().numpy()
     b = batch.GrainSet(gv, off, u0).refine(0.05, 3)[0].cpu().numpy()
     assert np.array_equal(a, b)
+
+
+def test_refine_csr_compensated_fp32(grains, oracle, cuda):
+    """The compensated-FP32 variant: FP32 screening inside the proven band
+    with an FP64 recheck (peak membership exact), normal equations summed as
+    compensated FP32 pairs (about FP64 accuracy), FP64 3x3 solves.  UBIs to
+    1e-9 relative."""
+    from imaged11_b200 import batch
+    gv, off, u0 = grains
+    ref_u, ref_n, ref_m = oracle.refine_csr(u0, gv, off, 0.05, 5)
+    gs = batch.GrainSet(gv, off, u0)
+    u, npk, mean = gs.refine(0.05, 5, precision="f32c")
+    u, npk, mean = u.cpu().numpy(), npk.cpu().numpy(), mean.cpu().numpy()
+    assert np.array_equal(npk, ref_n)
+    scale = np.abs(ref_u).reshape(len(ref_u), -1).max(1)
+    err = np.abs(u - ref_u).reshape(len(ref_u), -1).max(1)
+    assert np.all(err <= 1e-9 * scale), err.max()
+    # the mean drlv2 is a sum of FP32 per-peak values (each within the
+    # screening band of the exact one): about 1e-6 relative here
+    assert np.all(np.abs(mean - ref_m) <= 1e-4 * np.abs(ref_m) + 1e-18)

@@ -83,7 +83,7 @@ _SIGNATURES = [
     ("id11b_dev_refine_csr", _i, [_p, _p, _p, _p, _i, _d, _i, _i, _i, _p, _p, _p, _i64, _p]),
     ("id11b_dev_refine_csr_f32c", _i, [_p, _p, _p, _p, _i, _d, _i, _d, _p, _p, _p, _i64, _p]),
     ("id11b_dev_refine_translations", _i, [_p, _p, _p, _i, _p, _p, _d, _d, _d, _d, _d, _i, _p,
-                                            _p, _p]),
+                                            _p, _p, _p]),
     ("id11b_adjoint_workspace_bytes", _i64, [_i]),
     ("id11b_dev_residuals", _i, [_p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p, _p]),
     ("id11b_dev_residuals_adjoint", _i, [_p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p, _p,

@@ -495,14 +495,18 @@ class GrainSet:
 
 
 def refine_translations(xyz, omega, offsets, ubis, translations, omegasign, wavelength, wedge,
-                        chi, tol=1.0, iters=20):
+                        chi, tol=1.0, iters=20, ubis_refit=False):
     """Per-grain translations minimising the objective of
-    ImageD11/refinegrains.py refinepositions (the grain's UBI fixed, its
-    assigned peaks' drlv2 summed below tol^2 -- 1.0 there), for all grains in
-    one launch by damped Gauss-Newton.  xyz (n,3) lab positions and omega (n,)
-    sorted by grain, offsets (ngrains+1,), ubis (ngrains,3,3), translations
-    (ngrains,3) starting values.  Returns (translations, cost, npk) as CUDA
-    tensors; iters=0 only evaluates the objective."""
+    ImageD11/refinegrains.py refinepositions / gof: at each translation the
+    grain's g-vectors, one score_and_refine update of its UBI from the one
+    read (``ubis``), and the sum of drlv2 below tol^2 (1.0 there) at the
+    updated UBI.  All grains in one launch by damped Gauss-Newton.  xyz (n,3)
+    lab positions and omega (n,) sorted by grain, offsets (ngrains+1,), ubis
+    (ngrains,3,3), translations (ngrains,3) starting values.  Returns
+    (translations, cost, npk) as CUDA tensors -- refinegrains' gof of grain G
+    is 1e6 * cost[G] / npk[G] -- plus the updated UBIs (ngrains,3,3) at the
+    returned translations with ubis_refit=True; iters=0 only evaluates the
+    objective."""
     torch = _torch()
     x = _dev(xyz, torch.float64).reshape(-1, 3)
     om = _dev(omega, torch.float64).reshape(-1)
@@ -514,9 +518,14 @@ def refine_translations(xyz, omega, offsets, ubis, translations, omegasign, wave
         raise ValueError("refine_translations: inconsistent sizes")
     cost = torch.empty(ng, dtype=torch.float64, device=x.device)
     npk = torch.empty(ng, dtype=torch.int32, device=x.device)
+    u1 = torch.empty((ng, 3, 3), dtype=torch.float64, device=x.device) if ubis_refit else None
     check(lib.id11b_dev_refine_translations(x.data_ptr(), om.data_ptr(), off.data_ptr(), ng,
                                             u.data_ptr(), t.data_ptr(), float(omegasign),
                                             float(wavelength), float(wedge), float(chi),
                                             float(tol), int(iters), cost.data_ptr(),
-                                            npk.data_ptr(), _stream()), "refine_translations")
+                                            npk.data_ptr(),
+                                            u1.data_ptr() if u1 is not None else None,
+                                            _stream()), "refine_translations")
+    if ubis_refit:
+        return t, cost, npk, u1
     return t, cost, npk

@@ -386,20 +386,24 @@ int id11b_dev_refine_csr_f32c(double *ubis, const double *gv, const int64_t *off
 
 /* Per-grain translation refinement: minimises, for every grain G at once, the
  * objective of ImageD11/refinegrains.py refinepositions / gof (:517-560,
- * :639-660): the sum over grain G's peaks with drlv2 < tol^2 of
- * |UBI_G.g - round(UBI_G.g)|^2, g from compute_gv (src/cdiffraction.c:112-168)
- * at translation t_G, with UBI_G fixed -- by damped Gauss-Newton (analytic
- * 3x3 Jacobian per peak) where the reference runs a Nelder-Mead simplex per
- * grain.  Grain G owns xyz/omega rows offsets[G] .. offsets[G+1]-1 (lab
- * positions from compute_xlylzl, omega in degrees); translations (ngrains,3)
- * in/out; cost (optional) receives the final objective, npk (optional) the
- * peaks counted in it.  iters = 0 evaluates the objective at the given
- * translations only. */
+ * :636-660) -- by damped Gauss-Newton (analytic 3x3 Jacobian per peak) where
+ * the reference runs a Nelder-Mead simplex per grain.  At translation t_G the
+ * objective is what gof's refine (:459-498) computes: g from compute_gv
+ * (src/cdiffraction.c:112-168) at t_G, U1 = the score_and_refine update of
+ * UBI_G (least squares over the peaks with drlv2 < tol^2, hkl rounded at
+ * UBI_G), and cost = sum over the peaks with drlv2(U1) < tol^2 of
+ * |U1.g - round(U1.g)|^2, npk their count (refinegrains' gof is
+ * 1e6 * cost / npk).  Grain G owns xyz/omega rows offsets[G] ..
+ * offsets[G+1]-1 (lab positions from compute_xlylzl, omega in degrees);
+ * ubis (ngrains,9) are the UBIs read (left unchanged); translations
+ * (ngrains,3) in/out; cost, npk and ubis_refit (ngrains,9, the U1 at the
+ * final translations) are optional outputs.  iters = 0 evaluates the
+ * objective at the given translations only. */
 int id11b_dev_refine_translations(const double *xyz, const double *omega,
                                   const int64_t *offsets, int32_t ngrains, const double *ubis,
                                   double *translations, double omegasign, double wvln,
                                   double wedge, double chi, double tol, int iters, double *cost,
-                                  int32_t *npk, void *stream);
+                                  int32_t *npk, double *ubis_refit, void *stream);
 
 /* Residuals of assigned peaks and their adjoint (no single reference
  * function: the forward model chains compute_xlylzl and compute_gv,

@@ -208,7 +208,7 @@ def test_fused_loss_equals_residual_autograd(golden, cuda):
     r = adjoint.residuals(p2, u2, peaks)
     L2 = 0.5 * (r * r).sum()
     L2.backward()
-    assert abs(float(L1) - float(L2)) <= 1e-12 * float(L2)
+    assert abs(float(L1.detach()) - float(L2.detach())) <= 1e-12 * float(L2.detach())
     assert _close(p1.grad.cpu().numpy(), p2.grad.cpu().numpy())
     assert np.allclose(u1.grad.cpu().numpy(), u2.grad.cpu().numpy(), rtol=1e-10, atol=1e-12)
 

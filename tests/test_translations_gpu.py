@@ -2,9 +2,10 @@
 against the oracle.
 
 The objective at given translations equals the reference's gof numerator:
-per grain, compute_gv at the grain's translation then score_and_refine of
-the fixed UBI at tol = 1 (n * mean drlv2), to the rounding of the GPU's
-sin/cos (1e-9 relative).  The Gauss-Newton result reaches the simulated
+per grain, compute_gv at the grain's translation, one score_and_refine update
+of the UBI read at tol = 1, then n * mean drlv2 of a second score_and_refine
+at the updated UBI (refinegrains.refine's two calls), to the rounding of the
+GPU's sin/cos (1e-9 relative).  The Gauss-Newton result reaches the simulated
 translations and a cost no higher than a Nelder-Mead simplex (the reference's
 method) run on the oracle's objective."""
 import numpy as np
@@ -28,7 +29,8 @@ def scene():
 def oracle_cost(oracle, xyz, om, ubi, t, geo):
     gv = oracle.compute_gv(xyz, om, geo["omegasign"], geo["wavelength"], geo["wedge"],
                            geo["chi"], np.asarray(t, float))
-    n, mean, _ = oracle.score_and_refine(ubi, gv, 1.0)
+    _, _, u1 = oracle.score_and_refine(ubi, gv, 1.0)
+    n, mean, _ = oracle.score_and_refine(u1, gv, 1.0)
     return n * mean, n
 
 

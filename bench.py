@@ -39,9 +39,10 @@ sys.path.insert(0, REPO)
 TOLS = [0.02, 0.05, 0.1]
 # DRAM bytes (read + write) of one binned-join launch on this workload, from an ncu
 # capture of the same command (profiles/): the traffic is the box records
-K_JOIN_DRAM_BYTES = 401.2e6
+K_JOIN_DRAM_BYTES = 403.7e6
 K_JOIN_TRAFFIC_NOTE = ("dram__bytes_read.sum + dram__bytes_write.sum of one k_join<3> launch "
-                       "(20,000 UBIs, cell factor 0.8, x cut 8x; ncu capture named in "
+                       "(396.8 + 7.0 MB; 20,000 UBIs, cell factor 0.8, x cut 4x, the tuned "
+                       "shape; ncu --set full capture in "
                        "profiles/k_join_binned_20000ubi_1.1Mg.md): mostly the box records, "
                        "read once; the staged g come from L2")
 N_GRAINS = 2000
@@ -550,6 +551,12 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
                               xsubs=(2, 4, 8), reps=1)
     state.update(cs=base.cs * shape[0], xsub=shape[1])
     del base
+    # the binned join's workspace for the tuned shape, sized before the timed
+    # run (untimed setup, as the workspace a caller keeps between scans)
+    g_t = batch.GvecGrid(gv, cell=state["cs"], xsub=state["xsub"])
+    state["boxes"] = batch.bins_box_estimate(ub_d, g_t, tol)
+    state["ws"] = batch.BinsWorkspace(len(trials), g_t, state["boxes"])
+    del g_t
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
     run(ev, shape)
     names = ["compute_xlylzl+compute_gv", "cell_index+score_grid", "score_and_assign",
@@ -572,7 +579,8 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
            "value": pairs / (device_ms * 1e-3), "unit": "pairs/s",
            "assigned_peaks": out["assigned"], "peaks_per_grain_median": out["npk_median"],
            "geometry_step": out["geometry_step"],
-           "index_shape": {"cell_factor": shape[0], "xsub": shape[1]},
+           "index_shape": {"cell_factor": shape[0], "xsub": shape[1],
+                           "method": tune.grid_method(n)},
            "score_batch_fp32_ms": e0.elapsed_time(e1),
            "score_grid_counts_equal_fp32": bool(torch.equal(c32, cbuf)),
            "trial_counts_median_max": [int(cbuf[:, 0].median().item()),
@@ -1093,7 +1101,7 @@ def run_ours(args, rank, world, local_rank):
                               "rebuilt from the g-vectors in every step",
                        index_shape={"cell_factor": shape[0], "xsub": shape[1],
                                     "cell_A^-1": grid.cs, "nx": grid.nx}),
-        "tuning_ms": {"%g,%d" % t_: round(ms, 3) for t_, ms in grid_table},
+        "tuning_ms": {"%g,%d,%s" % t_: round(ms, 3) for t_, ms in grid_table},
         "e2e": {"value": e2e_value, "unit": "pairs/s",
                 "h2d_bytes_per_step": int(ps.gv.nbytes + ubis.nbytes),
                 "d2h_bytes_per_step": int(m * T * 4)},

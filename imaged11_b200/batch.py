@@ -251,19 +251,23 @@ def score_grid(ubis, grid, tols, sums=False, workspace=None, out=None, method=No
     sums=True, FP64 sums of the counted drlv2) for every UBI and tolerance,
     testing only the g-vectors near each UB.hkl.  grid: GvecGrid.
 
-    method "bins" (the default when every tolerance is below 0.4): the binned
-    join, every (UBI, hkl) box against the g of its bin's region in FP32 with
-    the proven FP64 recheck band (its sums' last bits depend on the order of
-    the atomics); "walk": per-box lookups with every candidate evaluated in
-    FP64 (any tolerance, sums in a fixed order).  workspace: a BinsWorkspace
-    ("bins") or a uint8 CUDA tensor ("walk")."""
+    method "bins": the binned join, every (UBI, hkl) box against the g of its
+    bin's region in FP32 with the proven FP64 recheck band (tolerances below
+    0.4; its sums' last bits depend on the order of the atomics); "walk":
+    per-box lookups with every candidate evaluated in FP64 (any tolerance,
+    sums in a fixed order).  Both give the same counts.  None: the method
+    tune.tune_grid found fastest for this many g-vectors, else "bins" where it
+    applies.  workspace: a BinsWorkspace ("bins") or a uint8 CUDA tensor
+    ("walk")."""
     torch = _torch()
     u = _dev(ubis, torch.float64).reshape(-1, 9)
     m = u.shape[0]
     t = _tols(tols)
     auto = method is None
     if auto:
-        method = "bins" if float(t.max()) < BINS_TOL_LIMIT and bins_fit(grid) else "walk"
+        from . import tune
+        bins_ok = float(t.max()) < BINS_TOL_LIMIT and bins_fit(grid)
+        method = "bins" if bins_ok and tune.grid_method(grid.n) != "walk" else "walk"
     elif method == "bins" and not bins_fit(grid):
         raise ValueError("the binned join holds at most %d rows of %d x cells; use "
                          "method='walk' or coarser cells" % (BINS_MAX_ROWS, BINS_MAX_XCELLS))

@@ -58,8 +58,14 @@ constexpr int kEW = 8;              // warps per enumeration CTA
 constexpr int kET = 32 * kEW;
 constexpr int kJT = 256;            // threads per join CTA (one row at a time)
 constexpr int kJW = kJT / 32;
-constexpr int kBMax = 4096;         // boxes of a row sorted in shared memory at a time
-constexpr int kGMax = 1536;         // g staged at a time (one tile)
+#ifndef ID11B_JOIN_BMAX
+#define ID11B_JOIN_BMAX 4096
+#endif
+#ifndef ID11B_JOIN_GMAX
+#define ID11B_JOIN_GMAX 1536
+#endif
+constexpr int kBMax = ID11B_JOIN_BMAX;  // boxes of a row sorted in shared memory at a time
+constexpr int kGMax = ID11B_JOIN_GMAX;  // g staged at a time (one tile)
 constexpr int kRowBlock = 16;       // rows of cells per block of the enumeration's streams
 constexpr int kMaxBlocks = 4096;    // blocks the enumeration's counters hold (nx^2 <= 65536)
 constexpr int kMaxNxx = 8191;       // x cells per row (13-bit field of a box record)

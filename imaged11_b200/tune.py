@@ -157,9 +157,12 @@ def tune_grid(ubis, gv, tols, cell_factors=(0.8, 1.0, 1.25), xsubs=(1, 2, 4, 8),
               method=None):
     """Time score_grid on these inputs for cell-index shapes: y/z cell side =
     factor x the default (about one g per cell of the bounding cube) and x cut
-    xsub times finer; cache the fastest per g-count bucket (GvecGrid uses it
-    when built without explicit shape) and return ((factor, xsub), table).
-    method: score_grid's method (None: its default for these tolerances)."""
+    xsub times finer, and for its two methods; cache the fastest shape and
+    method per g-count bucket (GvecGrid uses the shape when built without an
+    explicit one, score_grid the method when called without one) and return
+    ((factor, xsub), table of ((factor, xsub, method), ms)).  method: time
+    only that score_grid method ("bins" or "walk"; None: both, "bins" where
+    the tolerances and the shape allow it)."""
     from . import batch
     torch = _torch()
     g = batch._dev(gv, torch.float64).reshape(-1, 3)
@@ -173,22 +176,22 @@ def tune_grid(ubis, gv, tols, cell_factors=(0.8, 1.0, 1.25), xsubs=(1, 2, 4, 8),
             grid = batch.GvecGrid(g, cell=base.cs * f, xsub=xs)
             if grid.xsub != xs:
                 continue  # over the cell budget
-            m = method
-            if m is None:
-                m = "bins" if float(t.max()) < batch.BINS_TOL_LIMIT and batch.bins_fit(grid) \
-                    else "walk"
-            if m == "bins" and not batch.bins_fit(grid):
-                continue
-            ws = batch.BinsWorkspace(u.shape[0], grid, batch.bins_box_estimate(
-                u, grid, float(t.max()))) if m == "bins" else None
-            ms = _time(lambda: batch.score_grid(u, grid, t, out=out, method=m, workspace=ws),
-                       reps)
-            table.append(((f, xs), ms))
-            del grid, ws
+            bins_ok = float(t.max()) < batch.BINS_TOL_LIMIT and batch.bins_fit(grid)
+            methods = ["bins", "walk"] if method is None else [method]
+            for m in methods:
+                if m == "bins" and not bins_ok:
+                    continue
+                ws = batch.BinsWorkspace(u.shape[0], grid, batch.bins_box_estimate(
+                    u, grid, float(t.max()))) if m == "bins" else None
+                ms = _time(lambda: batch.score_grid(u, grid, t, out=out, method=m,
+                                                    workspace=ws), reps)
+                table.append(((f, xs, m), ms))
+                del ws
+            del grid
     best = min(table, key=lambda x: x[1])[0]
     _cache[grid_key(g.shape[0])] = list(best)
     _autosave()
-    return best, table
+    return best[:2], table
 
 
 def grid_shape(n):
@@ -196,7 +199,14 @@ def grid_shape(n):
     if not _cache:
         return None
     t = _cache.get(grid_key(n))
-    return tuple(t) if t else None
+    return tuple(t[:2]) if t else None
+
+
+def grid_method(n):
+    """The tuned score_grid method ("bins" or "walk") for this many
+    g-vectors, or None."""
+    t = _cache.get(grid_key(n)) if _cache else None
+    return t[2] if t and len(t) > 2 else None
 
 
 def save(path):

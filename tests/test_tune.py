@@ -100,7 +100,10 @@ def test_grid_tuner(tune, oracle, cuda):
     ubis = synth.trial_ubis(ps.ubis, 500, 0.1, 0.5, rng)
     tols = [0.05, 0.1]
     best, table = tune.tune_grid(ubis, ps.gv, tols, reps=1)
-    assert best in [t for t, _ in table]
+    assert best in [t[:2] for t, _ in table]
+    fastest = min(table, key=lambda x: x[1])[0]
+    assert {t[2] for t, _ in table} == {"bins", "walk"}  # both methods timed
+    assert tune.grid_method(len(ps.gv)) == fastest[2]
     grid = batch.GvecGrid(ps.gv)                      # picks the tuned shape
     assert grid.xsub == best[1]
     ref = oracle.score_many(ubis, ps.gv, tols)

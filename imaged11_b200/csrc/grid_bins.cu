@@ -58,6 +58,9 @@ constexpr int kEW = 8;              // warps per enumeration CTA
 constexpr int kET = 32 * kEW;
 constexpr int kJT = 256;            // threads per join CTA (one row at a time)
 constexpr int kJW = kJT / 32;
+#ifndef ID11B_JOIN_RANKED
+#define ID11B_JOIN_RANKED 1
+#endif
 #ifndef ID11B_JOIN_BMAX
 #define ID11B_JOIN_BMAX 4096
 #endif
@@ -96,8 +99,11 @@ struct BinInfo {
 // Everything the join needs that is uniform over the launch, computed on the
 // host after the counting pass (kernel parameters: no registers).
 struct JoinParams {
+    // thresholds in ascending order of tolerance; ord[j]: the caller's index
+    // of the j-th (where its count and sum are written)
     float lo[ID11B_MAX_TOLS], hi[ID11B_MAX_TOLS];
     double t2[ID11B_MAX_TOLS];
+    int ord[ID11B_MAX_TOLS];
     float hmax;
     // y/z region of row (iy, iz): [rlo + iy * cs, rhi + (iy + 1) * cs] (the
     // cell widened by W + eps; eps covers the FP32 rounding of the box
@@ -216,7 +222,10 @@ __device__ __forceinline__ void make_plan32(const volatile WarpPlan* wp, const H
 // them).  The mode is a run-time argument of one kernel, so both passes run
 // the same machine code and put every box in the same block; each write is
 // still bounded by the capacity of the box array.
-__global__ void __launch_bounds__(kET)
+#ifndef ID11B_ENUM_MINB
+#define ID11B_ENUM_MINB 1
+#endif
+__global__ void __launch_bounds__(kET, ID11B_ENUM_MINB)
 k_enum(int mode, const double* __restrict__ ubis, int64_t i0, int64_t mc, int64_t per,
        const Header* __restrict__ Hp, const int* __restrict__ start, double tmax, int first,
        int nblk, BinInfo* __restrict__ info, float4* __restrict__ packs,
@@ -383,6 +392,10 @@ k_blk_offsets(int* __restrict__ cta_blk, int nctas, int nblk, int* __restrict__ 
 constexpr int kRS = 512;
 constexpr int kRSW = kRS / 32;
 constexpr int kRK = 8;
+#ifndef ID11B_RS_PER_SM
+#define ID11B_RS_PER_SM 4
+#endif
+constexpr int kRSPerSM = ID11B_RS_PER_SM;  // row-split CTAs per SM (blocks in flight)
 
 __global__ void __launch_bounds__(kRS)
 k_rowsplit(const uint64_t* __restrict__ tmp, const int* __restrict__ blkstart, int nblk,
@@ -489,7 +502,13 @@ struct Staged {  // the tile of staged g, structure of arrays (pairs read as 64 
 // (an odd tile ends with a NaN g): testing g beyond a run's range is harmless,
 // every g of a tile being tested at most once per box.  Counting is free of
 // branches; one branch per pair of g catches the rare band cases.
-template <int NT, bool SUMS>
+//
+// RANKED (lo and hi both non-decreasing in j): a value below lo_j is below
+// every later lo, so the only band it can lie in is that of the largest lo_j
+// not above it -- one select chain and one compare instead of a test per
+// tolerance.  (If s lies in band i <= J, J the largest j with lo_j <= s, then
+// s < hi_i <= hi_J.)
+template <int NT, bool SUMS, bool RANKED>
 __device__ __forceinline__ void test_range(const Staged& t, int ga, int gb, const uint64_t uu[9],
                                            const uint64_t hh[3], const float* hkf,
                                            const JoinParams& P, const double* __restrict__ ubis,
@@ -509,6 +528,22 @@ __device__ __forceinline__ void test_range(const Staged& t, int ga, int gb, cons
         if (SUMS) {
             ra = sa < P.hmax;
             rb = sb < P.hmax;
+        } else if (RANKED) {
+            bool ia[NT], ib[NT];
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                ia[j] = sa < P.lo[j];
+                ib[j] = sb < P.lo[j];
+                cnt[j] += (int)ia[j] + (int)ib[j];
+            }
+            float ha = P.hi[NT - 1], hb = P.hi[NT - 1];
+#pragma unroll
+            for (int j = NT - 2; j >= 0; j--) {
+                ha = ia[j + 1] ? P.hi[j] : ha;
+                hb = ib[j + 1] ? P.hi[j] : hb;
+            }
+            ra = !ia[0] && sa < ha;
+            rb = !ib[0] && sb < hb;
         } else {
             ra = rb = false;
 #pragma unroll
@@ -557,7 +592,7 @@ __device__ __forceinline__ void block_scan(const int* a, int* b, int len, int* s
 // tiles of at most kGMax, each sorted by x cell, and every run of 32 sorted
 // boxes (one warp) is tested against the staged g in the x cells its boxes
 // can reach.
-template <int NT, bool SUMS>
+template <int NT, bool SUMS, bool RANKED>
 __global__ void __launch_bounds__(kJT, kJoinMinBlocks)
 k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nrows,
        int nhalo, BinInfo* __restrict__ info, const float4* __restrict__ packs,
@@ -751,12 +786,12 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
                             cnt[j] = 0;
                             sum[j] = 0.;
                         }
-                        test_range<NT, SUMS>(T, ga, gb, uu, hh, hkf, P, ubis, ubi, gs, cnt, sum,
-                                             ntest);
+                        test_range<NT, SUMS, RANKED>(T, ga, gb, uu, hh, hkf, P, ubis, ubi, gs,
+                                                     cnt, sum, ntest);
 #pragma unroll
                         for (int j = 0; j < NT; j++) {
-                            if (cnt[j]) atomicAdd(counts + ubi * NT + j, cnt[j]);
-                            if (SUMS && cnt[j]) atomicAdd(sums + ubi * NT + j, sum[j]);
+                            if (cnt[j]) atomicAdd(counts + ubi * NT + P.ord[j], cnt[j]);
+                            if (SUMS && cnt[j]) atomicAdd(sums + ubi * NT + P.ord[j], sum[j]);
                         }
                     }
                 }
@@ -857,17 +892,32 @@ k_special(const double* __restrict__ ubis, int64_t m, const double* __restrict__
     }
 }
 
-template <int NT, bool SUMS>
-int launch_join(int grid, size_t smem, const uint64_t* recs, const int* rstart, int nrows,
-                int nhalo, BinInfo* info, const float4* packs, const double* ubis, Header* H,
-                const int* start, const double* gs, const float4* g4, const JoinParams& P,
-                int* counts, double* sums, cudaStream_t st) {
-    ID11B_CHECK(cudaFuncSetAttribute(k_join<NT, SUMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-    k_join<NT, SUMS><<<grid, kJT, smem, st>>>(recs, rstart, nrows, nhalo, info, packs, ubis, H,
-                                              start, gs, g4, P, counts, sums);
+template <int NT, bool SUMS, bool RANKED>
+int launch_join_k(int grid, size_t smem, const uint64_t* recs, const int* rstart, int nrows,
+                  int nhalo, BinInfo* info, const float4* packs, const double* ubis, Header* H,
+                  const int* start, const double* gs, const float4* g4, const JoinParams& P,
+                  int* counts, double* sums, cudaStream_t st) {
+    ID11B_CHECK(cudaFuncSetAttribute(k_join<NT, SUMS, RANKED>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_join<NT, SUMS, RANKED><<<grid, kJT, smem, st>>>(recs, rstart, nrows, nhalo, info, packs,
+                                                      ubis, H, start, gs, g4, P, counts, sums);
     ID11B_CHECK_LAUNCH();
     return ID11B_OK;
+}
+
+// the ranked test where it applies (no sums, at least two tolerances, the
+// thresholds monotone); the per-tolerance test otherwise
+template <int NT, bool SUMS>
+int launch_join(int grid, size_t smem, bool ranked, const uint64_t* recs, const int* rstart,
+                int nrows, int nhalo, BinInfo* info, const float4* packs, const double* ubis,
+                Header* H, const int* start, const double* gs, const float4* g4,
+                const JoinParams& P, int* counts, double* sums, cudaStream_t st) {
+    if (!SUMS && NT > 1 && ranked)
+        return launch_join_k<NT, SUMS, !SUMS && NT != 1>(grid, smem, recs, rstart, nrows, nhalo,
+                                                         info, packs, ubis, H, start, gs, g4, P,
+                                                         counts, sums, st);
+    return launch_join_k<NT, SUMS, false>(grid, smem, recs, rstart, nrows, nhalo, info, packs,
+                                          ubis, H, start, gs, g4, P, counts, sums, st);
 }
 
 template <int NT, bool SUMS>
@@ -902,7 +952,11 @@ int ctas_per_sm(K kernel, int threads, size_t smem) {
 }
 
 template <int NT, bool SUMS>
-int join_ctas(size_t smem) { return ctas_per_sm(k_join<NT, SUMS>, kJT, smem); }
+int join_ctas(size_t smem, bool ranked) {
+    if (!SUMS && NT > 1 && ranked)
+        return ctas_per_sm(k_join<NT, SUMS, !SUMS && NT != 1>, kJT, smem);
+    return ctas_per_sm(k_join<NT, SUMS, false>, kJT, smem);
+}
 
 // float nearest to x in the given direction (x itself when representable)
 float float_rd(double x) {
@@ -1050,21 +1104,30 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     // the screening kernel's band (score_batch.cu) for gmax = G and the largest
     // row sum of the binned UBIs; the region geometry
     JoinParams P;
+    bool ranked = false;
     {
         const double G = -hh.lo;
         float smax;
         memcpy(&smax, &bi.smax_bits, sizeof(smax));
         const double E = 6.0 * kEps32 * (double)smax * G;
         P.hmax = 0.f;
+        // ascending order of tolerance (stable), unused slots last
+        int ord[ID11B_MAX_TOLS];
+        for (int j = 0; j < ID11B_MAX_TOLS; j++) ord[j] = j;
+        std::stable_sort(ord, ord + ntol, [&](int a, int b) { return T.t[a] < T.t[b]; });
         for (int j = 0; j < ID11B_MAX_TOLS; j++) {
-            const double t = T.t[j], TT = t * t;
+            const double t = T.t[ord[j]], TT = t * t;
             const double band = 1.25 * (3.0 * E * (2.0 * (t + 1e-3) + E) +
                                         4.0 * kEps32 * (TT + 0.01));
             P.lo[j] = float_rd(TT - band);
             P.hi[j] = float_ru(TT + band);
             P.t2[j] = TT;
+            P.ord[j] = ord[j];
             if (j < ntol) P.hmax = fmaxf(P.hmax, P.hi[j]);
         }
+        ranked = ID11B_JOIN_RANKED != 0;
+        for (int j = 1; j < ntol; j++)
+            ranked = ranked && P.lo[j] >= P.lo[j - 1] && P.hi[j] >= P.hi[j - 1];
         double W;
         memcpy(&W, &bi.wmax_bits, sizeof(W));
         // eps: far above the FP32 rounding of the box centres' cells (about
@@ -1084,7 +1147,7 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     const size_t jsmem = sizeof(uint64_t) * kBMax + 4 * sizeof(float) * kGMax +
                          4 * sizeof(int) * (size_t)(std::max(nxx, nhalo) + 1) +
                          2 * sizeof(int) * (size_t)(nhalo + 1);
-    const int jgrid = num_sms() * ID11B_BINS_DISPATCH(join_ctas, jsmem);
+    const int jgrid = num_sms() * ID11B_BINS_DISPATCH(join_ctas, jsmem, ranked);
     cudaEvent_t ev0 = t_join_start, ev1 = t_join_stop;
     t_join_start = t_join_stop = nullptr;
     bool ev0_done = false;
@@ -1102,8 +1165,8 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
         if (rc) return rc;
         enumerate(1, i0, mc, 0);
         ID11B_CHECK_LAUNCH();
-        k_rowsplit<<<(unsigned)std::min(nblk, num_sms() * 4), kRS, 0, st>>>(tmp, blkstart, nblk,
-                                                                           nrows, rstart, recs);
+        k_rowsplit<<<(unsigned)std::min(nblk, num_sms() * kRSPerSM), kRS, 0, st>>>(
+            tmp, blkstart, nblk, nrows, rstart, recs);
         ID11B_CHECK_LAUNCH();
         ID11B_CHECK(cudaMemsetAsync(&info->next_row, 0, sizeof(int), st));
         P.i0 = i0;
@@ -1111,8 +1174,8 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
             ID11B_CHECK(cudaEventRecord(ev0, st));
             ev0_done = true;
         }
-        rc = ID11B_BINS_DISPATCH(launch_join, jgrid, jsmem, recs, rstart, nrows, nhalo, info,
-                                 packs, ubis, H, start, gs, g4, P, counts, sums, st);
+        rc = ID11B_BINS_DISPATCH(launch_join, jgrid, jsmem, ranked, recs, rstart, nrows, nhalo,
+                                 info, packs, ubis, H, start, gs, g4, P, counts, sums, st);
         if (rc) return rc;
     }
     if (ev1) {

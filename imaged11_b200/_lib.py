@@ -85,12 +85,13 @@ _SIGNATURES = [
     ("id11b_dev_refine_translations", _i, [_p, _p, _p, _i, _p, _p, _d, _d, _d, _d, _d, _i, _p,
                                             _p, _p, _p]),
     ("id11b_adjoint_workspace_bytes", _i64, [_i]),
-    ("id11b_dev_residuals", _i, [_p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p, _p]),
-    ("id11b_dev_residuals_adjoint", _i, [_p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p, _p,
-                                          _i64, _p]),
-    ("id11b_dev_residual_loss", _i, [_p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p, _p, _p,
-                                      _i64, _p]),
-    ("id11b_dev_best_ubis", _i, [_p, _p, _p, _p, _p, _p, _p, _i, _p, _p]),
+    ("id11b_dev_residuals", _i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p, _p]),
+    ("id11b_dev_residuals_adjoint", _i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p,
+                                          _p, _i64, _p]),
+    ("id11b_dev_residual_loss", _i, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p, _p,
+                                      _p, _i64, _p]),
+    ("id11b_dev_best_ubis", _i, [_p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _p]),
+    ("id11b_dev_omega_sincos", _i, [_p, _i64, _d, _p, _p]),
     ("id11b_dev_bragg_theta", _i, [_p, _p, _p, _i, _d, _p, _p, _p]),
     ("id11b_dev_bragg_theta_adjoint", _i, [_p, _p, _p, _i, _d, _p, _p, _p]),
 ]

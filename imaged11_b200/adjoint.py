@@ -76,10 +76,16 @@ class PeakTable:
         self.det = np.array([float(geo[k]) for k in DETECTOR], dtype=np.float64)
         self.ws = torch.empty(lib.id11b_adjoint_workspace_bytes(max(self.ngrains, 1)) // 8,
                               dtype=torch.float64, device=dev)
+        # sin and cos of every peak's omega, made once: omega is fixed, so an
+        # optimiser's evaluations reuse them
+        self.omega_sincos = torch.empty((max(self.n, 1), 2), dtype=torch.float64, device=dev)
+        check(lib.id11b_dev_omega_sincos(self.omega.data_ptr(), self.n, self.omegasign,
+                                         self.omega_sincos.data_ptr(), _stream()), "omega_sincos")
 
     def _ptrs(self):
         return (self.det.ctypes.data, self.sc.data_ptr(), self.fc.data_ptr(),
-                self.omega.data_ptr(), self.hkl.data_ptr(), self.offsets.data_ptr())
+                self.omega.data_ptr(), self.omega_sincos.data_ptr(), self.hkl.data_ptr(),
+                self.offsets.data_ptr())
 
 
 def _stream():

@@ -40,6 +40,8 @@
 // fit), then the loss and geometry gradient are taken at that UBI.  At the
 // least-squares UBI dL/dUBI = 0, so the gradient of the projected loss with
 // respect to the geometry equals the partial derivative computed here.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace id11b {
@@ -61,7 +63,7 @@ struct AdjGeom {
 };
 
 struct PeakState {
-    double so, co, u[3], v1, v2, dh[3], n, k[3], g[3];
+    double so, co, u[3], v1, v2, dh[3], rn, k[3], g[3];  // rn = 1 / |d|
 };
 
 __device__ __forceinline__ void mat3mul(const double* a, const double* b, double* c) {
@@ -140,16 +142,31 @@ __device__ void make_geom(const double* p, const AdjDet& D, AdjGeom& P) {
     P.omegasign = D.omegasign;
 }
 
-__device__ __forceinline__ void forward_peak(const AdjGeom& P, double s, double f, double om,
-                                             PeakState& q) {
-    const double rad = 3.14159265358979323846 / 180.0;
+// sin and cos of the peak's omega * omegasign: from the table made by
+// id11b_dev_omega_sincos when one is given (omega is fixed for a peak, so
+// an optimiser's evaluations need not repeat them), else computed here
+__device__ __forceinline__ void peak_sincos(const AdjGeom& P, const double* __restrict__ omega,
+                                            const double* __restrict__ osc, int64_t kk,
+                                            double& so, double& co) {
+    if (osc) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(osc) + kk);
+        so = v.x;
+        co = v.y;
+    } else {
+        sincos(3.14159265358979323846 / 180.0 * omega[kk] * P.omegasign, &so, &co);
+    }
+}
+
+__device__ __forceinline__ void forward_peak(const AdjGeom& P, double s, double f, double so,
+                                             double co, PeakState& q) {
+    q.so = so;
+    q.co = co;
     q.v1 = (f - P.y_center) * P.y_size;
     q.v2 = (s - P.z_center) * P.z_size;
     double xyz[3];
 #pragma unroll
     for (int j = 0; j < 3; j++) xyz[j] = P.r[3 * j + 1] * q.v1 + P.r[3 * j + 2] * q.v2;
     xyz[0] += P.distance;
-    sincos(rad * om * P.omegasign, &q.so, &q.co);
     q.u[0] = q.co * P.t[0] - q.so * P.t[1];
     q.u[1] = q.so * P.t[0] + q.co * P.t[1];
     q.u[2] = P.t[2];
@@ -157,9 +174,11 @@ __device__ __forceinline__ void forward_peak(const AdjGeom& P, double s, double 
 #pragma unroll
     for (int i = 0; i < 3; i++)
         d[i] = xyz[i] - (P.M[3 * i] * q.u[0] + P.M[3 * i + 1] * q.u[1] + P.M[3 * i + 2] * q.u[2]);
-    q.n = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    q.rn = 1.0 / sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
 #pragma unroll
-    for (int i = 0; i < 3; i++) q.dh[i] = d[i] / q.n;
+    for (int i = 0; i < 3; i++) q.dh[i] = d[i] * q.rn;
+    // divided, not multiplied by a rounded 1/wavelength: the rounding then
+    // stays independent from peak to peak as wavelength varies
     q.k[0] = (q.dh[0] - 1.0) / P.wavelength;
     q.k[1] = q.dh[1] / P.wavelength;
     q.k[2] = q.dh[2] / P.wavelength;
@@ -203,7 +222,7 @@ __device__ __forceinline__ void adjoint_peak(const AdjGeom& P, const PeakState& 
     const double dd = q.dh[0] * adh[0] + q.dh[1] * adh[1] + q.dh[2] * adh[2];
     double ad[3];
 #pragma unroll
-    for (int i = 0; i < 3; i++) ad[i] = (adh[i] - q.dh[i] * dd) / q.n;
+    for (int i = 0; i < 3; i++) ad[i] = (adh[i] - q.dh[i] * dd) * q.rn;
     // o = M u: dM[i][j] += a_o_i u_j with a_o = -a_d
 #pragma unroll
     for (int i = 0; i < 3; i++)
@@ -252,6 +271,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kAT)
 k_residual(const double* __restrict__ params, AdjDet D, const double* __restrict__ sc,
            const double* __restrict__ fc, const double* __restrict__ omega,
+           const double* __restrict__ osc,
            const double* __restrict__ hkl, const int64_t* __restrict__ off,
            const double* __restrict__ ubis, int ngrains, double* __restrict__ res,
            double* __restrict__ gout, double* __restrict__ ssq,
@@ -277,7 +297,9 @@ k_residual(const double* __restrict__ params, AdjDet D, const double* __restrict
             for (int e = 0; e < 15; e++) a[e] = 0.;
             for (int64_t kk = k0 + tid; kk < k1; kk += kAT) {
                 PeakState q;
-                forward_peak(P, sc[kk], fc[kk], omega[kk], q);
+                double so, co;
+                peak_sincos(P, omega, osc, kk, so, co);
+                forward_peak(P, sc[kk], fc[kk], so, co, q);
                 const double h[3] = {hkl[3 * kk], hkl[3 * kk + 1], hkl[3 * kk + 2]};
 #pragma unroll
                 for (int i = 0; i < 3; i++)
@@ -331,7 +353,9 @@ k_residual(const double* __restrict__ params, AdjDet D, const double* __restrict
         for (int e = 0; e < NA; e++) acc[e] = 0.;
         for (int64_t kk = k0 + tid; kk < k1; kk += kAT) {
             PeakState q;
-            forward_peak(P, sc[kk], fc[kk], omega[kk], q);
+            double so, co;
+            peak_sincos(P, omega, osc, kk, so, co);
+            forward_peak(P, sc[kk], fc[kk], so, co, q);
             if (MODE == 0) {
                 if (gout) {
 #pragma unroll
@@ -481,6 +505,18 @@ k_bragg(const double* __restrict__ ubs, const double* __restrict__ hkl,
     }
 }
 
+// sin and cos of omega * omegasign (degrees) per peak, interleaved
+__global__ void k_omega_sincos(const double* __restrict__ omega, int64_t n, double omegasign,
+                               double* __restrict__ out) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        double so, co;
+        sincos(3.14159265358979323846 / 180.0 * omega[k] * omegasign, &so, &co);
+        out[2 * k] = so;
+        out[2 * k + 1] = co;
+    }
+}
+
 static int adj_grid(int ngrains) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
@@ -510,33 +546,40 @@ extern "C" int64_t id11b_adjoint_workspace_bytes(int32_t ngrains) {
     return (int64_t)sizeof(double) * kPart * (ngrains > 0 ? ngrains : 1);
 }
 
+// omega_sincos (optional, 16-byte aligned): the table id11b_dev_omega_sincos
+// makes for these peaks; NULL computes sin and cos of omega in the kernels
+static bool osc_misaligned(const double* osc) { return osc && ((uintptr_t)osc & 15); }
+
 extern "C" int id11b_dev_residuals(const double* params, const double* detector,
                                    const double* sc, const double* fc, const double* omega,
-                                   const double* hkl, const int64_t* offsets,
-                                   const double* ubis, int32_t ngrains, double* res,
-                                   double* gvec, double* ssq, void* stream) {
+                                   const double* omega_sincos, const double* hkl,
+                                   const int64_t* offsets, const double* ubis, int32_t ngrains,
+                                   double* res, double* gvec, double* ssq, void* stream) {
     AdjDet D;
     if (!params || adj_det(detector, D) || ngrains < 0) return ID11B_ERR_ARG;
+    if (osc_misaligned(omega_sincos)) return ID11B_ERR_ALIGN;
     if (ngrains == 0) return ID11B_OK;
     if (!offsets || !sc || !fc || !omega) return ID11B_ERR_ARG;
     if (ubis && (!hkl || !res)) return ID11B_ERR_ARG;
     if (!ubis && !gvec) return ID11B_ERR_ARG;
     k_residual<0><<<adj_grid(ngrains), kAT, 0, (cudaStream_t)stream>>>(
-        params, D, sc, fc, omega, hkl, offsets, ubis, ngrains, res, gvec, ubis ? ssq : nullptr,
-        nullptr, nullptr, nullptr, nullptr);
+        params, D, sc, fc, omega, omega_sincos, hkl, offsets, ubis, ngrains, res, gvec,
+        ubis ? ssq : nullptr, nullptr, nullptr, nullptr, nullptr);
     ID11B_CHECK_LAUNCH();
     return ID11B_OK;
 }
 
 extern "C" int id11b_dev_residuals_adjoint(const double* params, const double* detector,
                                            const double* sc, const double* fc,
-                                           const double* omega, const double* hkl,
-                                           const int64_t* offsets, const double* ubis,
-                                           int32_t ngrains, const double* grad_res,
-                                           double* grad_ubis, double* grad_params,
-                                           void* workspace, int64_t ws_bytes, void* stream) {
+                                           const double* omega, const double* omega_sincos,
+                                           const double* hkl, const int64_t* offsets,
+                                           const double* ubis, int32_t ngrains,
+                                           const double* grad_res, double* grad_ubis,
+                                           double* grad_params, void* workspace,
+                                           int64_t ws_bytes, void* stream) {
     AdjDet D;
     if (!params || adj_det(detector, D) || ngrains < 0 || !grad_params) return ID11B_ERR_ARG;
+    if (osc_misaligned(omega_sincos)) return ID11B_ERR_ALIGN;
     cudaStream_t st = (cudaStream_t)stream;
     if (ngrains == 0) {
         ID11B_CHECK(cudaMemsetAsync(grad_params, 0, sizeof(double) * kNP, st));
@@ -546,9 +589,10 @@ extern "C" int id11b_dev_residuals_adjoint(const double* params, const double* d
         return ID11B_ERR_ARG;
     if (ws_bytes < id11b_adjoint_workspace_bytes(ngrains)) return ID11B_ERR_SIZE;
     double* partial = (double*)workspace;
-    k_residual<1><<<adj_grid(ngrains), kAT, 0, st>>>(params, D, sc, fc, omega, hkl, offsets,
-                                                     ubis, ngrains, nullptr, nullptr, nullptr,
-                                                     grad_res, grad_ubis, partial, nullptr);
+    k_residual<1><<<adj_grid(ngrains), kAT, 0, st>>>(params, D, sc, fc, omega, omega_sincos, hkl,
+                                                     offsets, ubis, ngrains, nullptr, nullptr,
+                                                     nullptr, grad_res, grad_ubis, partial,
+                                                     nullptr);
     ID11B_CHECK_LAUNCH();
     k_finish<<<1, 32 * kPart, 0, st>>>(partial, ngrains, params, D, grad_params, nullptr);
     ID11B_CHECK_LAUNCH();
@@ -557,14 +601,15 @@ extern "C" int id11b_dev_residuals_adjoint(const double* params, const double* d
 
 extern "C" int id11b_dev_residual_loss(const double* params, const double* detector,
                                        const double* sc, const double* fc, const double* omega,
-                                       const double* hkl, const int64_t* offsets,
-                                       const double* ubis, int32_t ngrains, double* loss,
-                                       double* grad_ubis, double* grad_params,
-                                       double* ubis_out, void* workspace, int64_t ws_bytes,
-                                       void* stream) {
+                                       const double* omega_sincos, const double* hkl,
+                                       const int64_t* offsets, const double* ubis,
+                                       int32_t ngrains, double* loss, double* grad_ubis,
+                                       double* grad_params, double* ubis_out, void* workspace,
+                                       int64_t ws_bytes, void* stream) {
     AdjDet D;
     if (!params || adj_det(detector, D) || ngrains < 0 || !loss) return ID11B_ERR_ARG;
     if (!ubis && grad_ubis) return ID11B_ERR_ARG;
+    if (osc_misaligned(omega_sincos)) return ID11B_ERR_ALIGN;
     cudaStream_t st = (cudaStream_t)stream;
     if (ngrains == 0) {
         ID11B_CHECK(cudaMemsetAsync(loss, 0, sizeof(double), st));
@@ -576,12 +621,12 @@ extern "C" int id11b_dev_residual_loss(const double* params, const double* detec
     double* partial = (double*)workspace;
     const int grid = adj_grid(ngrains);
     if (ubis)
-        k_residual<2><<<grid, kAT, 0, st>>>(params, D, sc, fc, omega, hkl, offsets, ubis,
-                                            ngrains, nullptr, nullptr, nullptr, nullptr,
+        k_residual<2><<<grid, kAT, 0, st>>>(params, D, sc, fc, omega, omega_sincos, hkl, offsets,
+                                            ubis, ngrains, nullptr, nullptr, nullptr, nullptr,
                                             grad_ubis, partial, nullptr);
     else
-        k_residual<3><<<grid, kAT, 0, st>>>(params, D, sc, fc, omega, hkl, offsets, nullptr,
-                                            ngrains, nullptr, nullptr, nullptr, nullptr,
+        k_residual<3><<<grid, kAT, 0, st>>>(params, D, sc, fc, omega, omega_sincos, hkl, offsets,
+                                            nullptr, ngrains, nullptr, nullptr, nullptr, nullptr,
                                             nullptr, partial, ubis_out);
     ID11B_CHECK_LAUNCH();
     k_finish<<<1, 32 * kPart, 0, st>>>(partial, ngrains, params, D, grad_params, loss);
@@ -591,15 +636,17 @@ extern "C" int id11b_dev_residual_loss(const double* params, const double* detec
 
 extern "C" int id11b_dev_best_ubis(const double* params, const double* detector,
                                    const double* sc, const double* fc, const double* omega,
-                                   const double* hkl, const int64_t* offsets, int32_t ngrains,
-                                   double* ubis_out, void* stream) {
+                                   const double* omega_sincos, const double* hkl,
+                                   const int64_t* offsets, int32_t ngrains, double* ubis_out,
+                                   void* stream) {
     AdjDet D;
     if (!params || adj_det(detector, D) || ngrains < 0) return ID11B_ERR_ARG;
+    if (osc_misaligned(omega_sincos)) return ID11B_ERR_ALIGN;
     if (ngrains == 0) return ID11B_OK;
     if (!offsets || !sc || !fc || !omega || !hkl || !ubis_out) return ID11B_ERR_ARG;
     k_residual<4><<<adj_grid(ngrains), kAT, 0, (cudaStream_t)stream>>>(
-        params, D, sc, fc, omega, hkl, offsets, nullptr, ngrains, nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr, ubis_out);
+        params, D, sc, fc, omega, omega_sincos, hkl, offsets, nullptr, ngrains, nullptr,
+        nullptr, nullptr, nullptr, nullptr, nullptr, ubis_out);
     ID11B_CHECK_LAUNCH();
     return ID11B_OK;
 }
@@ -625,6 +672,19 @@ extern "C" int id11b_dev_bragg_theta_adjoint(const double* ubs, const double* hk
     if (!ubs || !hkl || !offsets || !grad_theta || !grad_ubs) return ID11B_ERR_ARG;
     k_bragg<true><<<adj_grid(ngrains), kAT, 0, (cudaStream_t)stream>>>(
         ubs, hkl, offsets, ngrains, wavelength, nullptr, nullptr, grad_theta, grad_ubs);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
+extern "C" int id11b_dev_omega_sincos(const double* omega, int64_t n, double omegasign,
+                                      double* sincos_out, void* stream) {
+    if (n < 0) return ID11B_ERR_ARG;
+    if (n == 0) return ID11B_OK;
+    if (!omega || !sincos_out) return ID11B_ERR_ARG;
+    if ((uintptr_t)sincos_out & 15) return ID11B_ERR_ALIGN;
+    const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 32);
+    k_omega_sincos<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(omega, n, omegasign,
+                                                                      sincos_out);
     ID11B_CHECK_LAUNCH();
     return ID11B_OK;
 }

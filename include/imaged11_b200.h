@@ -436,28 +436,36 @@ int id11b_dev_refine_translations(const double *xyz, const double *omega,
  * (sum h g^T)(sum g g^T)^-1 for the g-vectors at params; a grain whose
  * normal matrix B = sum g g^T is singular (det B <= 1e-10 trace(B)^3, as
  * for fewer than three independent g) gets UBI 0.
- * FP64; reductions in a fixed order (deterministic).  Workspace:
- * id11b_adjoint_workspace_bytes(ngrains). */
+ * omega_sincos (optional, NULL computes them): the table of
+ * id11b_dev_omega_sincos for the same peaks.  FP64; reductions in a fixed
+ * order (deterministic).  Workspace: id11b_adjoint_workspace_bytes(ngrains). */
 int64_t id11b_adjoint_workspace_bytes(int32_t ngrains);
 int id11b_dev_residuals(const double *params, const double *detector, const double *sc,
-                        const double *fc, const double *omega, const double *hkl,
-                        const int64_t *offsets, const double *ubis, int32_t ngrains,
-                        double *res, double *gvec, double *ssq, void *stream);
+                        const double *fc, const double *omega, const double *omega_sincos,
+                        const double *hkl, const int64_t *offsets, const double *ubis,
+                        int32_t ngrains, double *res, double *gvec, double *ssq, void *stream);
 int id11b_dev_residuals_adjoint(const double *params, const double *detector,
                                 const double *sc, const double *fc, const double *omega,
-                                const double *hkl, const int64_t *offsets, const double *ubis,
-                                int32_t ngrains, const double *grad_res, double *grad_ubis,
-                                double *grad_params, void *workspace, int64_t ws_bytes,
-                                void *stream);
+                                const double *omega_sincos, const double *hkl,
+                                const int64_t *offsets, const double *ubis, int32_t ngrains,
+                                const double *grad_res, double *grad_ubis, double *grad_params,
+                                void *workspace, int64_t ws_bytes, void *stream);
 int id11b_dev_residual_loss(const double *params, const double *detector, const double *sc,
-                            const double *fc, const double *omega, const double *hkl,
-                            const int64_t *offsets, const double *ubis, int32_t ngrains,
-                            double *loss, double *grad_ubis, double *grad_params,
-                            double *ubis_out, void *workspace, int64_t ws_bytes, void *stream);
+                            const double *fc, const double *omega, const double *omega_sincos,
+                            const double *hkl, const int64_t *offsets, const double *ubis,
+                            int32_t ngrains, double *loss, double *grad_ubis,
+                            double *grad_params, double *ubis_out, void *workspace,
+                            int64_t ws_bytes, void *stream);
 int id11b_dev_best_ubis(const double *params, const double *detector, const double *sc,
-                        const double *fc, const double *omega, const double *hkl,
-                        const int64_t *offsets, int32_t ngrains, double *ubis_out,
-                        void *stream);
+                        const double *fc, const double *omega, const double *omega_sincos,
+                        const double *hkl, const int64_t *offsets, int32_t ngrains,
+                        double *ubis_out, void *stream);
+/* sin and cos of omega * omegasign (omega in degrees) for n peaks,
+ * interleaved (2n doubles, 16-byte aligned): the omega_sincos table the
+ * residual entry points take, so that repeated evaluations over the same
+ * peaks do not recompute them. */
+int id11b_dev_omega_sincos(const double *omega, int64_t n, double omegasign,
+                           double *sincos_out, void *stream);
 
 /* Bragg angle of each assigned reflection computed from its grain's UB
  * matrix (ubs: ngrains x 9, row-major; hkl, offsets as above), in degrees,

@@ -253,7 +253,7 @@ def score_grid(ubis, grid, tols, sums=False, workspace=None, out=None, method=No
 
     method "bins": the binned join, every (UBI, hkl) box against the g of its
     bin's region in FP32 with the proven FP64 recheck band (tolerances below
-    0.4; its sums' last bits depend on the order of the atomics); "walk":
+    0.4; its FP64 sums accumulated in fixed point, reproducible); "walk":
     per-box lookups with every candidate evaluated in FP64 (any tolerance,
     sums in a fixed order).  Both give the same counts.  None: the method
     tune.tune_grid found fastest for this many g-vectors, else "bins" where it

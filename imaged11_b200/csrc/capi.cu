@@ -11,6 +11,24 @@
 static thread_local int t_last_status = ID11B_OK;
 static thread_local int t_last_cuda = 0;
 
+namespace {
+__global__ void k_fixsum_finish(double* __restrict__ sums, int64_t n, double inv_scale) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned long long q = reinterpret_cast<unsigned long long*>(sums)[i];
+        sums[i] = (double)q * inv_scale;
+    }
+}
+}  // namespace
+
+int id11b_fixsum_finish(double* sums, int64_t n, double scale, cudaStream_t st) {
+    if (!sums || n <= 0) return ID11B_OK;
+    const int64_t blocks = (n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096;
+    k_fixsum_finish<<<(unsigned)blocks, 256, 0, st>>>(sums, n, 1.0 / scale);
+    ID11B_CHECK_LAUNCH();
+    return ID11B_OK;
+}
+
 int id11b_record_cuda(cudaError_t e) {
     t_last_cuda = (int)e;
     return ID11B_ERR_CUDA;

@@ -1,6 +1,7 @@
 // Shared device helpers for the imaged11_b200 kernels (sm_100a).
 #pragma once
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 #include "../../include/imaged11_b200.h"
@@ -89,6 +90,25 @@ __device__ __forceinline__ void lsq_update_exact(double R[9], double H[9], doubl
     }
 }
 
+// Order-free sums of non-negative terms (drlv2): each term rounded to a
+// multiple of 1/scale and added as a 64-bit integer into the 8 bytes of its
+// double output slot (zeroed first), so that the total is the same whatever
+// order the atomics land in; id11b_fixsum_finish turns the slots back into
+// doubles.  fixsum_scale picks the largest power of two for which n terms
+// below tmax^2 cannot pass 2^62 (2^48 for 1.1M g at tol 0.1: a term is then
+// off by at most 2^-49).
+__device__ __forceinline__ void fixsum_add(double* slot, double x, double scale) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(slot), __double2ull_rn(x * scale));
+}
+inline double fixsum_scale(int64_t n, double tmax) {
+    const double t2 = tmax * tmax > 1e-300 ? tmax * tmax : 1e-300;
+    int e = 0;
+    frexp(4.611686018427387904e18 / ((double)(n > 0 ? n : 1) * t2), &e);  // 2^62 / worst
+    e -= 1;                                                                 // floor(log2)
+    e = e < 20 ? 20 : (e > 60 ? 60 : e);
+    return ldexp(1.0, e);
+}
+
 // Warp sums (fixed butterfly order, so results are reproducible run to run).
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -110,6 +130,9 @@ __device__ __forceinline__ long long warp_sum(long long v) {
 
 // Status from a launch: 0, or ID11B_ERR_CUDA with the CUDA code recorded.
 int id11b_record_cuda(cudaError_t e);
+// The n slots that fixsum_add accumulated with this scale, converted to
+// doubles in place.
+int id11b_fixsum_finish(double* sums, int64_t n, double scale, cudaStream_t st);
 #define ID11B_CHECK_LAUNCH()                                             \
     do {                                                                 \
         cudaError_t _e = cudaGetLastError();                             \

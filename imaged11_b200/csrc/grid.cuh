@@ -34,6 +34,7 @@ struct Header {
 
 struct Tols {
     double t[ID11B_MAX_TOLS];
+    double fix;  // fixed-point scale of order-free sums (fixsum_scale)
 };
 
 __host__ __device__ inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }

@@ -104,6 +104,7 @@ struct JoinParams {
     float lo[ID11B_MAX_TOLS], hi[ID11B_MAX_TOLS];
     double t2[ID11B_MAX_TOLS];
     int ord[ID11B_MAX_TOLS];
+    double fix;                    // fixed-point scale of the sums (fixsum_scale)
     float hmax;
     // y/z region of row (iy, iz): [rlo + iy * cs, rhi + (iy + 1) * cs] (the
     // cell widened by W + eps; eps covers the FP32 rounding of the box
@@ -479,7 +480,7 @@ template <int NT, bool SUMS>
 __device__ __forceinline__ void rare_pair(float s, int pos, const JoinParams& P,
                                           const double* __restrict__ ubis, int64_t ubi,
                                           const double* __restrict__ gs, const float* hkf,
-                                          int cnt[NT], double sum[NT]) {
+                                          int cnt[NT], unsigned long long sum[NT]) {
     const Exact e = exact_pair(ubis, ubi, gs, pos, hkf[0], hkf[1], hkf[2]);
     if (!e.own) return;
 #pragma unroll
@@ -487,7 +488,7 @@ __device__ __forceinline__ void rare_pair(float s, int pos, const JoinParams& P,
         if (!(e.s < P.t2[j])) continue;
         if (SUMS) {
             cnt[j]++;
-            sum[j] += e.s;
+            sum[j] += __double2ull_rn(e.s * P.fix);  // per term: order-free
         } else if (!(s < P.lo[j])) {
             cnt[j]++;
         }
@@ -516,7 +517,7 @@ __device__ __forceinline__ void test_range(const Staged& t, int ga, int gb, cons
                                            const uint64_t hh[3], const float* hkf,
                                            const JoinParams& P, const double* __restrict__ ubis,
                                            int64_t ubi, const double* __restrict__ gs, int cnt[NT],
-                                           double sum[NT], unsigned& ntest) {
+                                           unsigned long long sum[NT], unsigned& ntest) {
     for (int q = ga & ~1; q < gb; q += 2) {
         const uint64_t gx = *reinterpret_cast<const uint64_t*>(t.x + q);
         const uint64_t gy = *reinterpret_cast<const uint64_t*>(t.y + q);
@@ -783,18 +784,20 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
 #pragma unroll
                         for (int e = 0; e < 3; e++) hh[e] = pk2(hkf[e], hkf[e]);
                         int cnt[NT];
-                        double sum[NT];
+                        unsigned long long sum[NT];
 #pragma unroll
                         for (int j = 0; j < NT; j++) {
                             cnt[j] = 0;
-                            sum[j] = 0.;
+                            sum[j] = 0ull;
                         }
                         test_range<NT, SUMS, RANKED>(T, ga, gb, uu, hh, hkf, P, ubis, ubi, gs,
                                                      cnt, sum, ntest);
 #pragma unroll
                         for (int j = 0; j < NT; j++) {
                             if (cnt[j]) atomicAdd(counts + ubi * NT + P.ord[j], cnt[j]);
-                            if (SUMS && cnt[j]) atomicAdd(sums + ubi * NT + P.ord[j], sum[j]);
+                            if (SUMS && sum[j])
+                                atomicAdd(reinterpret_cast<unsigned long long*>(
+                                              sums + ubi * NT + P.ord[j]), sum[j]);
                         }
                     }
                 }
@@ -847,7 +850,7 @@ k_fallback(const double* __restrict__ ubis, const int* __restrict__ list, int nl
         const double sm = warp_sum(sum[j]);
         if (lane == 0 && c) {
             atomicAdd(counts + (int64_t)i * NT + j, c);
-            if (SUMS) atomicAdd(sums + (int64_t)i * NT + j, sm);
+            if (SUMS) fixsum_add(sums + (int64_t)i * NT + j, sm, tols.fix);
         }
     }
     if (part == 0 && lane == 0) atomicAdd(&Hp->nfallback, 1ull);
@@ -890,7 +893,7 @@ k_special(const double* __restrict__ ubis, int64_t m, const double* __restrict__
         const double sm = warp_sum(sum[j]);
         if (lane == 0 && c) {
             atomicAdd(counts + i * NT + j, c);
-            if (SUMS) atomicAdd(sums + i * NT + j, sm);
+            if (SUMS) fixsum_add(sums + i * NT + j, sm, tols.fix);
         }
     }
 }
@@ -1026,6 +1029,7 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
         if (!(tols_host[j] >= 0.) || !(tols_host[j] < kTolLimit)) return ID11B_ERR_ARG;
         tmax = fmax(tmax, tols_host[j]);
     }
+    T.fix = id11b::fixsum_scale(n, tmax);
     if (((uintptr_t)gridbuf & 255) || ((uintptr_t)ws & 255)) return ID11B_ERR_ALIGN;
     if (m > INT32_MAX - 1) return ID11B_ERR_SIZE;
     const int nrows = nx * nx;
@@ -1107,6 +1111,7 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     // the screening kernel's band (score_batch.cu) for gmax = G and the largest
     // row sum of the binned UBIs; the region geometry
     JoinParams P;
+    P.fix = T.fix;
     bool ranked = false;
     {
         const double G = -hh.lo;
@@ -1185,7 +1190,10 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
         if (!ev0_done) ID11B_CHECK(cudaEventRecord(ev0, st));
         ID11B_CHECK(cudaEventRecord(ev1, st));
     }
-    return ID11B_BINS_DISPATCH(launch_rest, ubis, m, fallback, bi.nfallback, H, start, gs, gv,
-                               (const int*)(g + L.spec), (const int*)(g + L.spos) + n,
-                               nspecial > 0, T, counts, sums, st);
+    const int rc = ID11B_BINS_DISPATCH(launch_rest, ubis, m, fallback, bi.nfallback, H, start,
+                                       gs, gv, (const int*)(g + L.spec),
+                                       (const int*)(g + L.spos) + n, nspecial > 0, T, counts,
+                                       sums, st);
+    if (rc) return rc;
+    return id11b_fixsum_finish(sums, m * ntol, T.fix, st);
 }

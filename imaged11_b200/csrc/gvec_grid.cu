@@ -923,6 +923,7 @@ extern "C" int id11b_dev_score_grid(const double* ubis, int64_t m, const double*
         (n > 0 && !gv))
         return ID11B_ERR_ARG;
     Tols T;
+    T.fix = 0.;  // the lookup's sums are fixed-order FP64
     for (int j = 0; j < ID11B_MAX_TOLS; j++) T.t[j] = j < ntol ? tols_host[j] : 0.;
     for (int j = 0; j < ntol; j++)
         if (!(tols_host[j] >= 0.) || !(tols_host[j] < 1e3)) return ID11B_ERR_ARG;

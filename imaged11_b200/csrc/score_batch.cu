@@ -83,6 +83,7 @@ struct UbiInfo {
 
 struct Tols {
     double t[ID11B_MAX_TOLS];
+    double fix;  // fixed-point scale of the sums (fixsum_scale)
 };
 
 struct LsqAcc {  // one UBI's normal-equation sums (same layout as the single-call path)
@@ -459,7 +460,7 @@ k_batch(const float4* __restrict__ packs, int64_t m, const float4* __restrict__ 
                 const int slot = j * (kBT * R) + r * kBT + tid;
                 if (s_cnt[slot]) {
                     atomicAdd(counts + mi[r] * NT + j, s_cnt[slot]);
-                    if (SUMS && sums) atomicAdd(sums + mi[r] * NT + j, (double)s_sum[slot]);
+                    if (SUMS && sums) fixsum_add(sums + mi[r] * NT + j, (double)s_sum[slot], tols.fix);
                 }
             }
         }
@@ -513,7 +514,7 @@ k_exact_lists(const double* __restrict__ ubis, int64_t m, const double* __restri
             for (int j = 0; j < ntol; j++)
                 if (s < tols.t[j] * tols.t[j]) {
                     atomicAdd(counts + ui_idx * ntol + j, 1);
-                    if (sums) atomicAdd(sums + ui_idx * ntol + j, s);
+                    if (sums) fixsum_add(sums + ui_idx * ntol + j, s, tols.fix);
                 }
         } else if (s < tols.t[0] * tols.t[0]) {
             LsqAcc* p = extra + ui_idx;
@@ -685,6 +686,7 @@ extern "C" int64_t id11b_batch_workspace_bytes(int64_t m, int64_t n, int refine)
 static int check_tols(const double* tols, int ntol, Tols& T) {
     if (!tols || ntol < 1 || ntol > ID11B_MAX_TOLS) return ID11B_ERR_ARG;
     for (int j = 0; j < ID11B_MAX_TOLS; j++) T.t[j] = j < ntol ? tols[j] : 0.;
+    T.fix = 0.;  // set where sums are accumulated
     for (int j = 0; j < ntol; j++)
         if (!(tols[j] >= 0.)) return ID11B_ERR_ARG;
     return ID11B_OK;
@@ -778,6 +780,7 @@ extern "C" int id11b_dev_score_batch_tiled(const double* ubis, int64_t m, const 
     if (sums && m > 0) ID11B_CHECK(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)m * ntol, st));
     double tmax = 0.;
     for (int j = 0; j < ntol; j++) tmax = tols_host[j] > tmax ? tols_host[j] : tmax;
+    T.fix = fixsum_scale(n, tmax);
     bool force = tmax >= kTolLimit;  // too close to the rounding half-point: all FP64
     rc = prepare_ubis(ubis, m, gws, w, force, st);
     if (rc) return rc;
@@ -795,7 +798,9 @@ extern "C" int id11b_dev_score_batch_tiled(const double* ubis, int64_t m, const 
                               sums, st);
 #endif
     ID11B_CHECK_LAUNCH();
-    return exact_lists(MODE_SCORE, ubis, m, gv, n, gws, w, T, ntol, counts, sums, nullptr, st);
+    rc = exact_lists(MODE_SCORE, ubis, m, gv, n, gws, w, T, ntol, counts, sums, nullptr, st);
+    if (rc) return rc;
+    return id11b_fixsum_finish(sums, m * ntol, T.fix, st);
 }
 
 extern "C" int id11b_dev_score_batch(const double* ubis, int64_t m, const double* gv,

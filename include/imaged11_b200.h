@@ -213,8 +213,9 @@ int64_t id11b_batch_workspace_bytes(int64_t m, int64_t n, int refine);
  * a proven error band of tol^2: counts identical to the reference's score()
  * (ImageD11 src/closest.c:227-248) for every (UBI, tol).  counts (m, ntol)
  * int32; sums (m, ntol) double, optional: sum of drlv2 of the counted pairs
- * (FP32 values, relative error below 1e-5).  ntol <= ID11B_MAX_TOLS; a
- * tolerance >= 0.45 sends every pair through exact FP64. */
+ * (FP32 values, relative error below 1e-5), accumulated in fixed point so
+ * that they repeat bit for bit.  ntol <= ID11B_MAX_TOLS; a tolerance >= 0.45
+ * sends every pair through exact FP64. */
 int id11b_dev_score_batch(const double *ubis, int64_t m, const double *gv, const float *g4,
                           int64_t n, const void *gws, const double *tols_host, int ntol,
                           int32_t *counts, double *sums, void *ws, int64_t ws_bytes,
@@ -286,8 +287,9 @@ int id11b_grid_stats(const void *gridbuf, int64_t *nregular, int64_t *nspecial,
  * with fewer bytes than the call needs, the UBIs are processed in ranges that
  * fit (ID11B_ERR_SIZE when one UBI's boxes alone do not fit).  The call reads
  * the box total back to the host (one stream synchronisation).  Sums, when
- * asked for, are added with double atomics: their last bits can differ
- * between runs; counts never do. */
+ * asked for, are of FP64 drlv2 values, accumulated in fixed point (steps of
+ * 2^-(62 - ceil(log2(n tmax^2))), 2^-49 for 1.1M g at tol 0.1) so that they
+ * repeat bit for bit; counts are exact. */
 int64_t id11b_grid_bins_workspace_bytes(int64_t m, int32_t nx, int32_t xsub, int64_t boxes);
 /* Measurement hook: the calling thread's next id11b_dev_score_grid_bins call
  * records start_event before its first join launch and stop_event after its

@@ -74,6 +74,9 @@ def test_scene_counts_and_sums(B, oracle, scene, cuda):
             assert n == c[i, j]
             bound = n * screening_band(ubis, ps.gv, t) + SUM_RTOL * mean * n
             assert abs(s[i, j] - mean * n) <= bound
+    # order-free (fixed-point) accumulation: the same sums, bit for bit
+    c2, s2 = B.score_batch(ubis, gs, tols, sums=True)
+    assert np.array_equal(c2.cpu().numpy(), c) and np.array_equal(s2.cpu().numpy(), s)
     nrecheck, nfallback = B.score_batch.last_workspace.stats()
     assert nfallback == 0
     assert nrecheck < 1e-3 * len(ubis) * len(ps.gv)

@@ -1,9 +1,10 @@
 // C ABI, layer 1: the reference's own C signatures with host pointers.
 //
-// Each call stages its inputs into device memory drawn from the stream-ordered
-// pool of the calling thread's per-thread default stream, runs the device
-// entry point and copies the results back before it returns.  Calls made from
-// different host threads use different streams and do not share buffers.
+// Each call stages its inputs into device memory on the calling thread's
+// per-thread default stream (buffers kept per thread and device for calls up
+// to 64 MB, the stream-ordered pool above that), runs the device entry point
+// and copies the results back before it returns.  Calls made from different
+// host threads use different streams and do not share buffers.
 #include <string.h>
 
 #include "common.cuh"
@@ -54,25 +55,96 @@ extern "C" int id11b_last_status(void) { return t_last_status; }
 
 namespace {
 
-// One pooled device allocation for the whole call, freed in stream order.
+// Calls of up to kKeepBytes stage through buffers kept per host thread and
+// device: a device buffer and a pinned host mirror of it, grown when a call
+// needs more.  Inputs are copied into the mirror and sent by DMA; outputs come
+// back into the mirror and are copied out after the call's one
+// synchronisation.  A small call then costs its launches and one round trip,
+// not an allocation and a pageable copy per array.  Larger calls draw one
+// allocation from the stream-ordered pool and copy pageable memory directly.
+constexpr size_t kKeepBytes = size_t(64) << 20;
+constexpr int kMaxDev = 64;
+
+struct ThreadBufs {
+    char* dev = nullptr;
+    char* pin = nullptr;
+    size_t cap = 0;
+    ~ThreadBufs() {  // at thread exit (the runtime may already be shutting down)
+        if (dev) cudaFree(dev);
+        if (pin) cudaFreeHost(pin);
+    }
+};
+thread_local ThreadBufs t_bufs[kMaxDev];
+thread_local int t_ndev = -1;
+
 struct Staging {
     cudaStream_t st = cudaStreamPerThread;
     char* base = nullptr;
+    char* pin = nullptr;  // mirror of base (kept buffers), else null
+    bool pooled = false;
     size_t used = 0, cap = 0;
     int status = ID11B_OK;
+    struct Out {
+        void* h;
+        size_t off, bytes;
+    };
+    static constexpr int kMaxOut = 8;
+    Out outs[kMaxOut];
+    int nout = 0;
     explicit Staging(size_t bytes) {
-        int ndev = 0;
-        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-            cudaGetLastError();
+        if (t_ndev < 0) {
+            int nd = 0;
+            if (cudaGetDeviceCount(&nd) != cudaSuccess) {
+                cudaGetLastError();
+                nd = 0;
+            }
+            t_ndev = nd;
+        }
+        if (t_ndev == 0) {
             status = ID11B_ERR_NODEV;
             return;
         }
         cap = bytes + 256 * 8;
-        cudaError_t e = cudaMallocAsync((void**)&base, cap, st);
-        if (e != cudaSuccess) status = id11b_record_cuda(e);
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) {
+            status = id11b_record_cuda(e);
+            return;
+        }
+        if (cap <= kKeepBytes && dev < kMaxDev) {
+            ThreadBufs& tb = t_bufs[dev];
+            if (tb.cap < cap) {
+                size_t want = tb.cap * 2 > cap ? tb.cap * 2 : cap;
+                want = want < (size_t(1) << 20) ? (size_t(1) << 20) : want;
+                want = want > kKeepBytes ? kKeepBytes : want;
+                if (tb.dev) cudaFree(tb.dev);
+                if (tb.pin) cudaFreeHost(tb.pin);
+                tb.dev = tb.pin = nullptr;
+                tb.cap = 0;
+                e = cudaMalloc((void**)&tb.dev, want);
+                if (e == cudaSuccess) e = cudaMallocHost((void**)&tb.pin, want);
+                if (e != cudaSuccess) {
+                    if (tb.dev) cudaFree(tb.dev);
+                    tb.dev = tb.pin = nullptr;
+                    status = id11b_record_cuda(e);
+                    return;
+                }
+                tb.cap = want;
+            }
+            base = tb.dev;
+            pin = tb.pin;
+            return;
+        }
+        e = cudaMallocAsync((void**)&base, cap, st);
+        if (e != cudaSuccess) {
+            base = nullptr;
+            status = id11b_record_cuda(e);
+            return;
+        }
+        pooled = true;
     }
     ~Staging() {
-        if (base) cudaFreeAsync(base, st);
+        if (pooled && base) cudaFreeAsync(base, st);
     }
     template <class T>
     T* take(size_t count) {
@@ -82,13 +154,48 @@ struct Staging {
     }
     int h2d(void* d, const void* h, size_t bytes) {
         if (status || !bytes) return status;
-        cudaError_t e = cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st);
+        cudaError_t e;
+        if (pin) {
+            const size_t off = (size_t)((char*)d - base);
+            memcpy(pin + off, h, bytes);
+            e = cudaMemcpyAsync(d, pin + off, bytes, cudaMemcpyHostToDevice, st);
+        } else {
+            e = cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st);
+        }
         if (e != cudaSuccess) status = id11b_record_cuda(e);
+        return status;
+    }
+    // put: copy into the pinned mirror now, send with the call's other inputs
+    // in one DMA over the range they span (send); without a mirror, copy now
+    size_t plo = ~(size_t)0, phi = 0;
+    int put(void* d, const void* h, size_t bytes) {
+        if (status || !bytes) return status;
+        if (!pin) return h2d(d, h, bytes);
+        const size_t off = (size_t)((char*)d - base);
+        memcpy(pin + off, h, bytes);
+        plo = off < plo ? off : plo;
+        phi = off + bytes > phi ? off + bytes : phi;
+        return status;
+    }
+    int send() {
+        if (status || phi == 0) return status;
+        cudaError_t e =
+            cudaMemcpyAsync(base + plo, pin + plo, phi - plo, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) status = id11b_record_cuda(e);
+        plo = ~(size_t)0;
+        phi = 0;
         return status;
     }
     int d2h(void* h, const void* d, size_t bytes) {
         if (status || !bytes) return status;
-        cudaError_t e = cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, st);
+        cudaError_t e;
+        if (pin && nout < kMaxOut) {
+            const size_t off = (size_t)((const char*)d - base);
+            e = cudaMemcpyAsync(pin + off, d, bytes, cudaMemcpyDeviceToHost, st);
+            outs[nout++] = Out{h, off, bytes};
+        } else {
+            e = cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, st);
+        }
         if (e != cudaSuccess) status = id11b_record_cuda(e);
         return status;
     }
@@ -97,9 +204,16 @@ struct Staging {
         return status;
     }
     int sync() {
-        if (status) return status;
+        if (status == ID11B_ERR_NODEV) return status;
+        // always drained, so that the kept buffers are idle when the call
+        // returns, whatever went wrong before
         cudaError_t e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) status = id11b_record_cuda(e);
+        if (status) return status;
+        if (e != cudaSuccess) {
+            status = id11b_record_cuda(e);
+            return status;
+        }
+        for (int i = 0; i < nout; i++) memcpy(outs[i].h, pin + outs[i].off, outs[i].bytes);
         return status;
     }
 };
@@ -110,23 +224,13 @@ int finish(Staging& s) {
     return s.status;
 }
 
-// Small results come back through one pinned buffer per host thread (a copy
-// from device to pageable memory costs a staging step per call).
+// The refined UBI, n and mean of one least-squares call, returned in one copy.
 struct LsqResult {
     double u[9];
     double mean;
     int32_t n;
     int32_t pad;
 };
-
-LsqResult* pinned_result() {
-    static thread_local LsqResult* r = nullptr;
-    if (!r && cudaMallocHost((void**)&r, sizeof(LsqResult)) != cudaSuccess) {
-        cudaGetLastError();
-        r = nullptr;
-    }
-    return r;
-}
 
 }  // namespace
 
@@ -138,8 +242,9 @@ extern "C" void id11b_compute_gv(double xlylzl[][3], double omega[], double omeg
     double* dx = s.take<double>(3 * (size_t)n);
     double* dom = s.take<double>(n);
     double* dg = s.take<double>(3 * (size_t)n);
-    s.h2d(dx, xlylzl, sizeof(double) * 3 * (size_t)n);
-    s.h2d(dom, omega, sizeof(double) * (size_t)n);
+    s.put(dx, xlylzl, sizeof(double) * 3 * (size_t)n);
+    s.put(dom, omega, sizeof(double) * (size_t)n);
+    s.send();
     if (!s.status)
         s.run(id11b_dev_compute_gv(dx, dom, omegasign, wvln, wedge, chi, t, dg, nullptr, n, s.st));
     s.d2h(gv, dg, sizeof(double) * 3 * (size_t)n);
@@ -154,8 +259,9 @@ extern "C" void id11b_compute_geometry(double xlylzl[][3], double omega[], doubl
     double* dx = s.take<double>(3 * (size_t)n);
     double* dom = s.take<double>(n);
     double* dout = s.take<double>(6 * (size_t)n);
-    s.h2d(dx, xlylzl, sizeof(double) * 3 * (size_t)n);
-    s.h2d(dom, omega, sizeof(double) * (size_t)n);
+    s.put(dx, xlylzl, sizeof(double) * 3 * (size_t)n);
+    s.put(dom, omega, sizeof(double) * (size_t)n);
+    s.send();
     if (!s.status)
         s.run(id11b_dev_compute_geometry(dx, dom, omegasign, wvln, wedge, chi, t, dout, n, s.st));
     s.d2h(out, dout, sizeof(double) * 6 * (size_t)n);
@@ -169,8 +275,9 @@ extern "C" void id11b_compute_xlylzl(double sl[], double f[], double p[4], doubl
     double* ds = s.take<double>(n);
     double* df = s.take<double>(n);
     double* dx = s.take<double>(3 * (size_t)n);
-    s.h2d(ds, sl, sizeof(double) * (size_t)n);
-    s.h2d(df, f, sizeof(double) * (size_t)n);
+    s.put(ds, sl, sizeof(double) * (size_t)n);
+    s.put(df, f, sizeof(double) * (size_t)n);
+    s.send();
     if (!s.status) s.run(id11b_dev_compute_xlylzl(ds, df, p, r, dist, dx, n, s.st));
     s.d2h(xlylzl, dx, sizeof(double) * 3 * (size_t)n);
     finish(s);
@@ -183,8 +290,9 @@ extern "C" int id11b_score(double ubi[3][3], double gv[][3], double tol, int ng)
     double* dg = s.take<double>(3 * (size_t)ng);
     int32_t* dc = s.take<int32_t>(1);
     int32_t count = -1;
-    s.h2d(du, ubi, sizeof(double) * 9);
-    s.h2d(dg, gv, sizeof(double) * 3 * (size_t)ng);
+    s.put(du, ubi, sizeof(double) * 9);
+    s.put(dg, gv, sizeof(double) * 3 * (size_t)ng);
+    s.send();
     if (!s.status) s.run(id11b_dev_score(du, dg, tol, ng, dc, s.st));
     s.d2h(&count, dc, sizeof(int32_t));
     return finish(s) ? -1 : count;
@@ -200,9 +308,10 @@ static void lsq_host(int mode, double ubi[3][3], double gv[][3], double tol, int
     double* dg = s.take<double>(3 * (size_t)ng);
     int32_t* dl = mode ? s.take<int32_t>(ng) : nullptr;
     char* ws = s.take<char>(wsb);
-    s.h2d(dr->u, ubi, sizeof(double) * 9);
-    s.h2d(dg, gv, sizeof(double) * 3 * (size_t)ng);
-    if (mode) s.h2d(dl, labels, sizeof(int32_t) * (size_t)ng);
+    s.put(dr->u, ubi, sizeof(double) * 9);
+    s.put(dg, gv, sizeof(double) * 3 * (size_t)ng);
+    if (mode) s.put(dl, labels, sizeof(int32_t) * (size_t)ng);
+    s.send();
     if (!s.status) {
         if (mode == 0)
             s.run(id11b_dev_score_and_refine(dr->u, dg, tol, ng, &dr->n, &dr->mean, ws, wsb,
@@ -211,14 +320,12 @@ static void lsq_host(int mode, double ubi[3][3], double gv[][3], double tol, int
             s.run(id11b_dev_refine_assigned(dr->u, dg, dl, label, ng, &dr->n, &dr->mean, ws, wsb,
                                             s.st));
     }
-    LsqResult local;
-    LsqResult* hr = pinned_result();
-    if (!hr) hr = &local;
-    s.d2h(hr, dr, sizeof(LsqResult));
+    LsqResult hr;
+    s.d2h(&hr, dr, sizeof(LsqResult));
     if (finish(s) == ID11B_OK) {
-        memcpy(ubi, hr->u, sizeof(hr->u));
-        *n_out = hr->n;
-        *mean_out = hr->mean;
+        memcpy(ubi, hr.u, sizeof(hr.u));
+        *n_out = hr.n;
+        *mean_out = hr.mean;
     }
 }
 
@@ -241,10 +348,11 @@ extern "C" int id11b_score_and_assign(double ubi[3][3], double gv[][3], double t
     double* dd = s.take<double>(ng);
     int32_t* dl = s.take<int32_t>(ng);
     int32_t* dc = s.take<int32_t>(1);
-    s.h2d(du, ubi, sizeof(double) * 9);
-    s.h2d(dg, gv, sizeof(double) * 3 * (size_t)ng);
-    s.h2d(dd, drlv2, sizeof(double) * (size_t)ng);
-    s.h2d(dl, labels, sizeof(int32_t) * (size_t)ng);
+    s.put(du, ubi, sizeof(double) * 9);
+    s.put(dg, gv, sizeof(double) * 3 * (size_t)ng);
+    s.put(dd, drlv2, sizeof(double) * (size_t)ng);
+    s.put(dl, labels, sizeof(int32_t) * (size_t)ng);
+    s.send();
     if (!s.status) s.run(id11b_dev_score_and_assign(du, dg, tol, dd, dl, label, ng, dc, s.st));
     int32_t count = -1;
     s.d2h(drlv2, dd, sizeof(double) * (size_t)ng);

@@ -22,6 +22,7 @@ namespace id11b {
 
 constexpr int kThreads = 256;
 constexpr int kLsqMaxBlocks = 1024;
+constexpr int64_t kLsqSingleMax = 16384;  // peaks scored by one CTA in one launch
 
 struct LsqPartial {
     double r[9];   // sum ih_j * g_i       (R, row-major)
@@ -57,18 +58,19 @@ k_score(const double* __restrict__ ubi, const double* __restrict__ gv, double to
 // Stage 1: per-CTA partial sums.  MODE 0 = score_and_refine (accept by tol),
 // MODE 1 = refine_assigned (accept by label).
 template <int MODE>
-__global__ void __launch_bounds__(kThreads)
-k_lsq_partials(const double* __restrict__ ubi, const double* __restrict__ gv, double tolsq,
-               const int* __restrict__ labels, int label, int64_t ng,
-               LsqPartial* __restrict__ part) {
+__device__ __forceinline__ void lsq_partials_body(const double* __restrict__ ubi,
+                                                  const double* __restrict__ gv, double tolsq,
+                                                  const int* __restrict__ labels, int label,
+                                                  int64_t ng, LsqPartial* __restrict__ part,
+                                                  int blk, int nblk) {
     double u[9];
     load_ubi(ubi, u);
     double r[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     double h[6] = {0, 0, 0, 0, 0, 0};
     double ss = 0.;
     long long n = 0;
-    for (int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x; k < ng;
-         k += (int64_t)gridDim.x * kThreads) {
+    for (int64_t k = (int64_t)blk * kThreads + threadIdx.x; k < ng;
+         k += (int64_t)nblk * kThreads) {
         if (MODE == 1 && __ldg(labels + k) != label) continue;
         double g0 = __ldg(gv + 3 * k), g1 = __ldg(gv + 3 * k + 1), g2 = __ldg(gv + 3 * k + 2);
         double ih[3];
@@ -114,22 +116,29 @@ k_lsq_partials(const double* __restrict__ ubi, const double* __restrict__ gv, do
                 const double* src = f < 9 ? s_w[q].r + f : (f < 15 ? s_w[q].h + (f - 9) : &s_w[q].ss);
                 acc += *src;
             }
-            double* dst = f < 9 ? part[blockIdx.x].r + f
-                                : (f < 15 ? part[blockIdx.x].h + (f - 9) : &part[blockIdx.x].ss);
+            double* dst = f < 9 ? part[blk].r + f : (f < 15 ? part[blk].h + (f - 9) : &part[blk].ss);
             *dst = acc;
         } else {
             long long acc = 0;
             for (int q = 0; q < kThreads / 32; q++) acc += s_w[q].n;
-            part[blockIdx.x].n = acc;
+            part[blk].n = acc;
         }
     }
 }
 
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+k_lsq_partials(const double* __restrict__ ubi, const double* __restrict__ gv, double tolsq,
+               const int* __restrict__ labels, int label, int64_t ng,
+               LsqPartial* __restrict__ part) {
+    lsq_partials_body<MODE>(ubi, gv, tolsq, labels, label, ng, part, blockIdx.x, gridDim.x);
+}
+
 // Stage 2: one CTA sums the partials in a fixed order and applies the
 // reference's least-squares update (ImageD11 src/closest.c:326-344).
-__global__ void __launch_bounds__(kThreads)
-k_lsq_finish(const LsqPartial* __restrict__ part, int nparts, double* __restrict__ ubi,
-             int* __restrict__ n_out, double* __restrict__ mean_out) {
+__device__ __forceinline__ void lsq_finish_body(const LsqPartial* __restrict__ part, int nparts,
+                                                double* __restrict__ ubi, int* __restrict__ n_out,
+                                                double* __restrict__ mean_out) {
     __shared__ double s_acc[kThreads / 32][16];
     __shared__ long long s_n[kThreads / 32];
     double acc[16];
@@ -174,6 +183,24 @@ k_lsq_finish(const LsqPartial* __restrict__ part, int nparts, double* __restrict
         *n_out = (int)nn;
         *mean_out = nn > 0 ? ddiv(t[15], (double)nn) : 0.;
     }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_lsq_finish(const LsqPartial* __restrict__ part, int nparts, double* __restrict__ ubi,
+             int* __restrict__ n_out, double* __restrict__ mean_out) {
+    lsq_finish_body(part, nparts, ubi, n_out, mean_out);
+}
+
+// Small inputs: both stages in one CTA and one launch (the partial sums of
+// one CTA, then the finish), so that a small call pays one kernel launch.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+k_lsq_single(double* __restrict__ ubi, const double* __restrict__ gv, double tolsq,
+             const int* __restrict__ labels, int label, int64_t ng, LsqPartial* __restrict__ part,
+             int* __restrict__ n_out, double* __restrict__ mean_out) {
+    lsq_partials_body<MODE>(ubi, gv, tolsq, labels, label, ng, part, 0, 1);
+    __syncthreads();  // part[0] written by this CTA
+    lsq_finish_body(part, 1, ubi, n_out, mean_out);
 }
 
 // ------------------------------------------------------- score_and_assign ----
@@ -310,6 +337,16 @@ static int lsq_launch(int mode, double* ubi, const double* gv, double tol,
     cudaStream_t st = (cudaStream_t)stream;
     LsqPartial* part = (LsqPartial*)ws;
     int nb = lsq_blocks(ng);
+    if (ng > 0 && ng <= kLsqSingleMax) {
+        if (mode == 0)
+            k_lsq_single<0><<<1, kThreads, 0, st>>>(ubi, gv, tol * tol, nullptr, 0, ng, part, n,
+                                                    mean);
+        else
+            k_lsq_single<1><<<1, kThreads, 0, st>>>(ubi, gv, 0., labels, label, ng, part, n,
+                                                    mean);
+        ID11B_CHECK_LAUNCH();
+        return ID11B_OK;
+    }
     if (ng == 0) {
         ID11B_CHECK(cudaMemsetAsync(part, 0, sizeof(LsqPartial), st));
     } else if (mode == 0) {

@@ -8,10 +8,12 @@
  *     pointers.  Each call copies its inputs to the GPU, runs the kernels and
  *     copies the results back before returning, so a binding that today points
  *     at ImageD11's src/closest.c / src/cdiffraction.c can point here instead.
- *     Device memory is taken from the CUDA stream-ordered pool on the calling
- *     thread's per-thread default stream, so concurrent calls from different
- *     host threads are safe (the reference marks score_and_refine and
- *     refine_assigned "threadsafe").
+ *     Calls run on the calling thread's per-thread default stream and stage
+ *     through device and pinned host buffers kept per host thread and device
+ *     (up to 64 MB, grown on demand and held until the thread exits; larger
+ *     calls draw from the CUDA stream-ordered pool), so concurrent calls from
+ *     different host threads are safe (the reference marks score_and_refine
+ *     and refine_assigned "threadsafe").
  *
  *  2. Device entry points (id11b_dev_<name>): DEVICE pointers for every array,
  *     scalars by value, small fixed-size parameter vectors (t[3], p[4], r[9],

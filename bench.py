@@ -548,8 +548,9 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
     # (untimed setup; the counts do not depend on it)
     from imaged11_b200 import tune
     base = batch.GvecGrid(gv, xsub=1)
-    shape, _ = tune.tune_grid(ub_d[::10], gv, [tol], cell_factors=(0.8, 1.0, 1.25),
-                              xsubs=(2, 4, 8), reps=1)
+    shape, ptable = tune.tune_grid(ub_d[::10], gv, [tol],
+                                   cell_factors=(0.8, 1.0, 1.25), xsubs=(2, 4, 8),
+                                   reps=1)
     state.update(cs=base.cs * shape[0], xsub=shape[1])
     del base
     # the binned join's workspace for the tuned shape, sized before the timed
@@ -581,7 +582,9 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
            "assigned_peaks": out["assigned"], "peaks_per_grain_median": out["npk_median"],
            "geometry_step": out["geometry_step"],
            "index_shape": {"cell_factor": shape[0], "xsub": shape[1],
-                           "method": tune.grid_method(n)},
+                           "method": tune.grid_method(n),
+                           "tuning_ms_tenth_of_trials": {"%g,%d,%s" % t_: round(ms, 2)
+                                                         for t_, ms in ptable}},
            "score_batch_fp32_ms": e0.elapsed_time(e1),
            "score_grid_counts_equal_fp32": bool(torch.equal(c32, cbuf)),
            "trial_counts_median_max": [int(cbuf[:, 0].median().item()),

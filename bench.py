@@ -39,9 +39,9 @@ sys.path.insert(0, REPO)
 TOLS = [0.02, 0.05, 0.1]
 # DRAM bytes (read + write) of one binned-join launch on this workload, from an ncu
 # capture of the same command (profiles/): the traffic is the box records
-K_JOIN_DRAM_BYTES = 403.7e6
+K_JOIN_DRAM_BYTES = 401.0e6
 K_JOIN_TRAFFIC_NOTE = ("dram__bytes_read.sum + dram__bytes_write.sum of one k_join<3> launch "
-                       "(396.8 + 7.0 MB; 20,000 UBIs, cell factor 0.8, x cut 4x -- the "
+                       "(397.1 + 3.9 MB; 20,000 UBIs, cell factor 0.8, x cut 4x -- the "
                        "autotuner picks 4x or 8x, within 1% of each other; ncu --set full "
                        "capture in "
                        "profiles/k_join_binned_20000ubi_1.1Mg.md): mostly the box records, "

@@ -204,3 +204,47 @@ def test_compute_gv_specialisations_and_nonfinite(cim, oracle, cuda):
         fin = np.isfinite(ref).all(1)
         assert np.array_equal(np.isinf(got), np.isinf(ref))
         assert _close_ulps(got[fin], ref[fin], GV_ULPS)
+
+
+def test_host_calls_small_large_and_threads(cim, oracle, cuda):
+    """Host-buffer calls stage through buffers kept per host thread (calls up to
+    64 MB) or the stream-ordered pool (larger): alternate small and large
+    calls, then run calls from four host threads at once; every result equals
+    the oracle's (counts exact, UBIs 1e-12)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from imaged11_b200 import synth
+    rng = np.random.default_rng(71)
+    nb = 1_600_000                                     # 38 MB of g, > 64 MB staged
+    big = np.stack([150000.0 + rng.normal(0, 100, nb), rng.uniform(-1e5, 1e5, nb),
+                    rng.uniform(-1e5, 1e5, nb)], axis=1)  # lab positions (um)
+    om = rng.uniform(-180, 180, nb)
+    ps = synth.simulate(4, "Al", gmax=1.0, seed=72)
+    ubis = [np.array(u, order="C") for u in ps.ubis]
+    g_big = np.empty_like(big)
+    cim.compute_gv(big, om, 1.0, 0.2846, 0.01, -0.02, [10.0, -20.0, 5.0], g_big)
+    ref = oracle.compute_gv(big, om, 1.0, 0.2846, 0.01, -0.02, np.array([10.0, -20.0, 5.0]))
+    assert _close_ulps(g_big, ref, GV_ULPS)
+    small = np.ascontiguousarray(g_big[:5000])
+    for g in (small, g_big, small, ps.gv):
+        for u in ubis:
+            assert cim.score(u, g, 0.05) == oracle.score(u, g, 0.05)
+            uu = u.copy()
+            n, m = cim.score_and_refine(uu, g, 0.05)
+            n2, m2, u2 = oracle.score_and_refine(u, g, 0.05)
+            assert n == n2 and abs(m - m2) <= 1e-12 * abs(m2)
+            assert np.abs(uu - u2).max() <= 1e-12 * np.abs(u2).max()
+
+    def work(k):
+        out = []
+        for rep in range(20):
+            u = ubis[(k + rep) % len(ubis)].copy()
+            out.append((cim.score_and_refine(u, ps.gv, 0.05), u))
+        return out
+
+    with ThreadPoolExecutor(4) as ex:
+        results = list(ex.map(work, range(4)))
+    for k, res in enumerate(results):
+        for rep, ((n, m), u) in enumerate(res):
+            n2, m2, u2 = oracle.score_and_refine(ubis[(k + rep) % len(ubis)], ps.gv, 0.05)
+            assert n == n2 and abs(m - m2) <= 1e-12 * abs(m2)
+            assert np.abs(u - u2).max() <= 1e-12 * np.abs(u2).max()

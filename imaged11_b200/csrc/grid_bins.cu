@@ -58,6 +58,9 @@ constexpr int kEW = 8;              // warps per enumeration CTA
 constexpr int kET = 32 * kEW;
 constexpr int kJT = 256;            // threads per join CTA (one row at a time)
 constexpr int kJW = kJT / 32;
+#ifndef ID11B_JOIN_FOLD
+#define ID11B_JOIN_FOLD 1
+#endif
 #ifndef ID11B_JOIN_RANKED
 #define ID11B_JOIN_RANKED 1
 #endif
@@ -522,10 +525,18 @@ __device__ __forceinline__ void test_range(const Staged& t, int ga, int gb, cons
         const uint64_t gx = *reinterpret_cast<const uint64_t*>(t.x + q);
         const uint64_t gy = *reinterpret_cast<const uint64_t*>(t.y + q);
         const uint64_t gz = *reinterpret_cast<const uint64_t*>(t.z + q);
+#if ID11B_JOIN_FOLD
+        // UBI.g - hkl with the subtraction folded into the first FMA (hh holds
+        // -hkl): three roundings of partial sums below |hkl| + S gmax
+        const uint64_t d0 = fma2(uu[2], gz, fma2(uu[1], gy, fma2(uu[0], gx, hh[0])));
+        const uint64_t d1 = fma2(uu[5], gz, fma2(uu[4], gy, fma2(uu[3], gx, hh[1])));
+        const uint64_t d2 = fma2(uu[8], gz, fma2(uu[7], gy, fma2(uu[6], gx, hh[2])));
+#else
         const uint64_t h0 = fma2(uu[2], gz, fma2(uu[1], gy, mul2(uu[0], gx)));
         const uint64_t h1 = fma2(uu[5], gz, fma2(uu[4], gy, mul2(uu[3], gx)));
         const uint64_t h2 = fma2(uu[8], gz, fma2(uu[7], gy, mul2(uu[6], gx)));
         const uint64_t d0 = sub2(h0, hh[0]), d1 = sub2(h1, hh[1]), d2 = sub2(h2, hh[2]);
+#endif
         float sa, sb;
         upk2(fma2(d2, d2, fma2(d1, d1, mul2(d0, d0))), sa, sb);
         bool ra, rb;
@@ -782,7 +793,8 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
 #pragma unroll
                         for (int e = 0; e < 9; e++) uu[e] = pk2(u[e], u[e]);
 #pragma unroll
-                        for (int e = 0; e < 3; e++) hh[e] = pk2(hkf[e], hkf[e]);
+                        for (int e = 0; e < 3; e++)
+                            hh[e] = ID11B_JOIN_FOLD ? pk2(-hkf[e], -hkf[e]) : pk2(hkf[e], hkf[e]);
                         int cnt[NT];
                         unsigned long long sum[NT];
 #pragma unroll
@@ -1117,7 +1129,16 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
         const double G = -hh.lo;
         float smax;
         memcpy(&smax, &bi.smax_bits, sizeof(smax));
-        const double E = 6.0 * kEps32 * (double)smax * G;
+        double W;
+        memcpy(&W, &bi.wmax_bits, sizeof(W));
+        // the FP32 error of the screened UBI.g - hkl per component: inputs
+        // rounded (2 eps S G) and three roundings, of partial sums below S G
+        // (h; the subtraction of hkl is then exact where it matters) or, folded,
+        // below |hkl| + S G <= S (2 G + W) (a box's centre c lies within G + W of
+        // the origin in every component, and hkl = UBI.c)
+        const double E = ID11B_JOIN_FOLD
+                             ? kEps32 * (double)smax * (8.0 * G + 3.0 * W) * (1. + 1e-6)
+                             : 6.0 * kEps32 * (double)smax * G;
         P.hmax = 0.f;
         // ascending order of tolerance (stable), unused slots last
         int ord[ID11B_MAX_TOLS];
@@ -1136,8 +1157,6 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
         ranked = ID11B_JOIN_RANKED != 0;
         for (int j = 1; j < ntol; j++)
             ranked = ranked && P.lo[j] >= P.lo[j - 1] && P.hi[j] >= P.hi[j - 1];
-        double W;
-        memcpy(&W, &bi.wmax_bits, sizeof(W));
         // eps: far above the FP32 rounding of the box centres' cells (about
         // 2^-23 of |c| + |lo|) and of the FP32 region bounds
         const double eps = 2e-5 * (1. + G);

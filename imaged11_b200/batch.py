@@ -177,9 +177,10 @@ class GvecGrid:
 
     def refresh(self):
         """Rebuild the index from self.gv (changed in place) into the same
-        buffer and shape, reading nothing back: every g must stay inside the
-        cube the index was sized for (|g_j| <= gmax; larger or non-finite g go
-        to the list of g outside the regular range, as at build)."""
+        buffer and shape, reading nothing back.  g that left the cube and ball
+        the index was sized for (|g_j| <= gmax, |g| <= rmax) go to the list of
+        g scored by a plain scan, as non-finite ones do: counts stay exact,
+        and a rebuild with fresh bounds restores the speed."""
         check(lib.id11b_dev_build_grid(self.gv.data_ptr(), self.n, self.gmax, self.rmax,
                                        self.cs, self.nx, self.xsub, self.buf.data_ptr(),
                                        self.buf.numel(), _stream()), "build_grid")

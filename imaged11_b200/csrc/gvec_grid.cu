@@ -22,7 +22,8 @@
 // box is always inside the scanned cells.  UBIs outside the caps (non-finite,
 // singular, ill-conditioned, or with more candidate hkl than g-vectors) are
 // scored by a plain scan of every regular g; g-vectors outside the regular
-// range (non-finite or |g_j| > 1024) by a scan over that list.
+// range (non-finite or |g_j| > 1024), or outside the cube and ball of radius
+// rmax the index was built for, by a scan over that list.
 #include "grid.cuh"
 
 namespace id11b {
@@ -72,7 +73,7 @@ k_count(const double* __restrict__ gv, int64_t n, const Header* __restrict__ Hp,
     for (int64_t k = (int64_t)blockIdx.x * kGT + threadIdx.x; k < n;
          k += (int64_t)gridDim.x * kGT) {
         double a = gv[3 * k], b = gv[3 * k + 1], c = gv[3 * k + 2];
-        const bool reg = regular(a, b, c);
+        const bool reg = indexed(a, b, c, H);
         flag[k] = reg ? 0 : 1;
         if (reg) atomicAdd(cnt + cell_of(a, b, c, H), 1);
     }
@@ -171,7 +172,7 @@ k_scatter(const double* __restrict__ gv, int64_t n, const Header* __restrict__ H
     for (int64_t k = (int64_t)blockIdx.x * kGT + threadIdx.x; k < n;
          k += (int64_t)gridDim.x * kGT) {
         double a = gv[3 * k], b = gv[3 * k + 1], c = gv[3 * k + 2];
-        if (!regular(a, b, c)) {
+        if (!indexed(a, b, c, H)) {
             spec[spos[k]] = (int)k;
             continue;
         }

@@ -240,9 +240,11 @@ int id11b_dev_score_batch_tiled(const double *ubis, int64_t m, const double *gv,
 /* Reciprocal-space cell index (no reference counterpart; it replaces the
  * reference's test of every g against every UBI in score(), ImageD11
  * src/closest.c:227-248, with a lookup of the g near each UB.hkl).
- * Regular g-vectors (finite, every |g_j| <= 1024) are binned into nx^3 cubic
- * cells of side cs over [-gmax, gmax]^3, sorted by cell (x fastest; within a
- * cell by index); the others are kept in an index list.
+ * Regular g-vectors (finite, every |g_j| <= 1024) inside [-gmax, gmax]^3 and
+ * within rmax of the origin are binned into nx^3 cubic cells of side cs over
+ * that cube, sorted by cell (x fastest; within a cell by index); the others
+ * are kept in an index list and scored by a plain scan (so bounds smaller
+ * than the data's cost speed, never counts).
  *   1. id11b_dev_gvec_bounds: bounds[0] = max |g_j|, bounds[1] = max |g| over
  *      regular g, as float bits rounded up (device, 2 x uint32);
  *   2. id11b_grid_plan (host): nx and cs for n g-vectors; cell = 0 picks about

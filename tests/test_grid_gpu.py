@@ -245,3 +245,97 @@ def test_bins_rejects_large_tolerances(B, scene, cuda):
     ps, ubis = scene
     with pytest.raises(Exception):
         B.score_grid(ubis[:4], B.GvecGrid(ps.gv[:100]), [0.1, 0.4], method="bins")
+
+
+def test_bins_unsorted_tolerances_and_large_hkl(B, oracle, scene, cuda):
+    """The join counts with the tolerances sorted and writes each count (and
+    sum) back to the caller's column: unsorted and repeated tolerances give the
+    reference's counts column by column, and sums equal to the lookup's to the
+    fixed-point step.  Cells elongated along one axis put h near +-250 (the
+    record's limit is 255) through the join, the widest FMA-chain error bound."""
+    ps, ubis = scene
+    tols = [0.1, 0.05, 0.35, 0.05]
+    grid = B.GvecGrid(ps.gv)
+    c, s = B.score_grid(ubis[:400], grid, tols, sums=True, method="bins")
+    cw, sw = B.score_grid(ubis[:400], grid, tols, sums=True, method="walk")
+    ref = oracle.score_many(ubis[:400], ps.gv, tols)
+    assert np.array_equal(c.cpu().numpy(), ref) and np.array_equal(cw.cpu().numpy(), ref)
+    step = 2.0 ** -(62 - np.ceil(np.log2(len(ps.gv) * max(tols) ** 2)))
+    diff = np.abs(s.cpu().numpy() - sw.cpu().numpy())
+    assert np.all(diff <= 1e-12 * sw.cpu().numpy() + ref * step), diff.max()
+    rng = np.random.default_rng(79)
+    g = rng.normal(size=(400000, 3))
+    g *= (1.5 * rng.uniform(size=(len(g), 1)) ** (1 / 3)) / np.linalg.norm(g, axis=1)[:, None]
+    grid = B.GvecGrid(g)   # more g than the elongated cells' candidate hkl
+    big = np.empty((60, 3, 3))
+    G = grid.gmax * (1 + 1e-6)       # the cube that bounds every |hkl| of the plan
+    for i in range(len(big)):
+        th, ph = rng.uniform(0, 2 * np.pi), rng.uniform(-0.05, 0.05)
+        rx = np.array([[1, 0, 0], [0, np.cos(th), -np.sin(th)], [0, np.sin(th), np.cos(th)]])
+        rz = np.array([[np.cos(ph), -np.sin(ph), 0], [np.sin(ph), np.cos(ph), 0], [0, 0, 1]])
+        m = (rz @ rx).T                                   # rows: the cell's axes
+        s0 = rng.uniform(0.85, 0.99) * 253.0 / (G * np.abs(m[0]).sum())
+        big[i] = np.diag([s0, *rng.uniform(2.0, 4.0, 2)]) @ m
+    hmax = np.abs(np.einsum("mij,nj->mni", big[:8], g[:20000])).max()
+    assert 150 < hmax < 255
+    for t in ([0.3, 0.1, 0.2], [0.05]):
+        c = B.score_grid(big, grid, t, method="bins").cpu().numpy()
+        assert grid.stats()["fallback_ubis"] == 0
+        assert np.array_equal(c, oracle.score_many(big, g, t)), t
+        assert c[:, 0].sum() > 0
+
+
+def _snap_to_cell_faces(grid, g, rng):
+    """g moved to the nearest face of the index's cells in each coordinate
+    (x faces every cs / xsub, y and z every cs, from the cube's corner lo),
+    then one ulp down, left, or one ulp up, at random per coordinate."""
+    lo = -(grid.gmax * (1. + 1e-6) + 1e-300)
+    side = np.array([grid.cs / grid.xsub, grid.cs, grid.cs])
+    q = lo + np.round((g - lo) / side) * side
+    which = rng.integers(0, 3, size=g.shape)
+    q = np.where(which == 1, np.nextafter(q, -np.inf),
+                 np.where(which == 2, np.nextafter(q, np.inf), q))
+    return np.clip(q, -grid.gmax, grid.gmax)
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_g_on_cell_faces(B, oracle, scene, method, cuda):
+    """g-vectors on the faces of the cells (and one ulp either side): the build
+    and every query take a g's cell from one monotone function, and the boxes
+    are widened past their rounding, so counts there are the reference's."""
+    import torch
+    ps, ubis = scene
+    rng = np.random.default_rng(31)
+    for cell, xsub in ((0.03, 4), (0.05, 1)):
+        grid = B.GvecGrid(ps.gv[:300000], cell=cell, xsub=xsub)
+        q = _snap_to_cell_faces(grid, ps.gv[:300000], rng)
+        grid.gv.copy_(torch.from_numpy(q))
+        grid.refresh()
+        assert grid.stats()["special"] < 0.01 * len(q)
+        tols = [0.05, 0.1, 0.2]
+        c = B.score_grid(ubis[:300], grid, tols, method=method).cpu().numpy()
+        assert np.array_equal(c, oracle.score_many(ubis[:300], q, tols)), (cell, xsub)
+        assert c[:, 1].sum() > 1000
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_g_outside_the_built_bounds(B, oracle, scene, method, cuda):
+    """A rebuild into the same shape after the g-vectors moved (refresh) keeps
+    the cube and rmax of the first build: g now outside them join the list
+    scored by a plain scan, so no box misses them and counts stay exact."""
+    import torch
+    ps, ubis = scene
+    g = ps.gv[:200000]
+    grid = B.GvecGrid(g)
+    assert grid.stats()["special"] == 0
+    moved = g * 1.08
+    grid.gv.copy_(torch.from_numpy(moved))
+    grid.refresh()
+    st = grid.stats()
+    outside = (np.abs(moved).max(axis=1) > grid.gmax) | \
+        (np.linalg.norm(moved, axis=1) > grid.rmax)
+    assert outside.sum() > 200 and st["special"] >= 0.99 * outside.sum()
+    assert st["regular"] + st["special"] == len(g)
+    tols = [0.05, 0.2]
+    c = B.score_grid(ubis[:300], grid, tols, method=method).cpu().numpy()
+    assert np.array_equal(c, oracle.score_many(ubis[:300], moved, tols))

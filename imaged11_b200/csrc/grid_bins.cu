@@ -54,7 +54,15 @@ namespace id11b {
 namespace grid {
 namespace bins {
 
-constexpr int kEW = 8;              // warps per enumeration CTA
+// warps per enumeration CTA, and CTAs per SM (ID11B_ENUM_MINB): every CTA
+// writes one stream of box records per block, so fewer, larger CTAs mean fewer
+// streams, each filling its L2 sectors sooner.  Binned scoring of 20,000 UBIs x
+// 1.1M g: 2.96 ms at 8 warps x 3 CTAs (444 CTAs), 2.88 at 12 x 2, 2.87 at
+// 16 x 1 (104 registers), 2.79 at 24 x 1 (80 registers).
+#ifndef ID11B_ENUM_WARPS
+#define ID11B_ENUM_WARPS 24
+#endif
+constexpr int kEW = ID11B_ENUM_WARPS;
 constexpr int kET = 32 * kEW;
 constexpr int kJT = 256;            // threads per join CTA (one row at a time)
 constexpr int kJW = kJT / 32;
@@ -72,7 +80,13 @@ constexpr int kJW = kJT / 32;
 #endif
 constexpr int kBMax = ID11B_JOIN_BMAX;  // boxes of a row sorted in shared memory at a time
 constexpr int kGMax = ID11B_JOIN_GMAX;  // g staged at a time (one tile)
-constexpr int kRowBlock = 16;       // rows of cells per block of the enumeration's streams
+// rows per block: 2^ID11B_ROW_BITS (blocks of 32 rows halve the streams but
+// were slower: 2.83 against 2.79 ms with 24-warp enumeration CTAs)
+#ifndef ID11B_ROW_BITS
+#define ID11B_ROW_BITS 4
+#endif
+constexpr int kRowBits = ID11B_ROW_BITS;
+constexpr int kRowBlock = 1 << kRowBits;  // rows of cells per block of the enumeration's streams
 constexpr int kMaxBlocks = 4096;    // blocks the enumeration's counters hold (nx^2 <= 65536)
 constexpr int kMaxNxx = 8191;       // x cells per row (13-bit field of a box record)
 constexpr int kMaxHalo = 1024;      // rows of cells around a row (the halo R: (2R+1)^2)
@@ -81,7 +95,11 @@ constexpr double kTolLimit = 0.4;
 constexpr double kSGLimit = 16384.0;
 constexpr double kEps32 = 5.9604644775390625e-08;  // 2^-24
 constexpr int kHklOff = 256;        // hkl in 9-bit fields: -256 .. 255
-constexpr int kUbiBits = 20;        // UBI index (within a range of UBIs) in a box record
+// box record fields above the 13-bit x cell: the row within its block, l, k,
+// h, then the UBI (within a range of UBIs) in what is left of the 64 bits
+constexpr int kLShift = 13 + kRowBits, kKShift = kLShift + 9, kHShift = kKShift + 9,
+              kUShift = kHShift + 9;
+constexpr int kUbiBits = 64 - kUShift;
 constexpr int kFallbackParts = 128; // warps per plainly scanned UBI
 constexpr int kBT = 128;            // threads per CTA of the exact scans
 constexpr int kBW = kBT / 32;
@@ -117,15 +135,17 @@ struct JoinParams {
     int64_t i0;                    // first UBI of the range (box records are relative to it)
 };
 
-// box record (64 bits): UBI (20 bits, relative to the range) | h + 256 (9) |
-// k + 256 (9) | l + 256 (9) | row within its block of 16 (4) | x cell (13)
+// box record (64 bits): UBI (kUbiBits, relative to the range) | h + 256 (9) |
+// k + 256 (9) | l + 256 (9) | row within its block (kRowBits) | x cell (13)
 __device__ __forceinline__ uint64_t pack_box(int64_t u, int h, int k, int l, int rowlo, int fx) {
-    return ((uint64_t)u << 44) | ((uint64_t)(h + kHklOff) << 35) |
-           ((uint64_t)(k + kHklOff) << 26) | ((uint64_t)(l + kHklOff) << 17) |
+    return ((uint64_t)u << kUShift) | ((uint64_t)(h + kHklOff) << kHShift) |
+           ((uint64_t)(k + kHklOff) << kKShift) | ((uint64_t)(l + kHklOff) << kLShift) |
            ((uint64_t)rowlo << 13) | (uint64_t)fx;
 }
 __device__ __forceinline__ int box_fx(uint64_t r) { return (int)(r & 8191u); }
-__device__ __forceinline__ int box_rowlo(uint64_t r) { return (int)((r >> 13) & 15u); }
+__device__ __forceinline__ int box_rowlo(uint64_t r) {
+    return (int)((r >> 13) & (uint64_t)(kRowBlock - 1));
+}
 
 struct BinLayout {
     size_t info, packs, cnt_ubi, fallback, cta_blk, blktot, blkstart, rstart, tot, tmp, recs,
@@ -226,10 +246,8 @@ __device__ __forceinline__ void make_plan32(const volatile WarpPlan* wp, const H
 // them).  The mode is a run-time argument of one kernel, so both passes run
 // the same machine code and put every box in the same block; each write is
 // still bounded by the capacity of the box array.
-// three CTAs per SM (80 registers, a few bytes spilled in the per-UBI setup):
-// binned scoring of 20,000 UBIs x 1.1M g 0.02 ms faster than two (104)
 #ifndef ID11B_ENUM_MINB
-#define ID11B_ENUM_MINB 3
+#define ID11B_ENUM_MINB 1
 #endif
 __global__ void __launch_bounds__(kET, ID11B_ENUM_MINB)
 k_enum(int mode, const double* __restrict__ ubis, int64_t i0, int64_t mc, int64_t per,
@@ -768,10 +786,10 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
                         npairs += (unsigned long long)nrun * (unsigned)(((gb + 1) & ~1) - (ga & ~1));
                     if (lane < nrun && ga < gb) {
                         const uint64_t rec = s_box[k0 + lane];
-                        const int64_t ubi = P.i0 + (int64_t)(rec >> 44);
-                        const float hkf[3] = {(float)((int)((rec >> 35) & 511) - kHklOff),
-                                              (float)((int)((rec >> 26) & 511) - kHklOff),
-                                              (float)((int)((rec >> 17) & 511) - kHklOff)};
+                        const int64_t ubi = P.i0 + (int64_t)(rec >> kUShift);
+                        const float hkf[3] = {(float)((int)((rec >> kHShift) & 511) - kHklOff),
+                                              (float)((int)((rec >> kKShift) & 511) - kHklOff),
+                                              (float)((int)((rec >> kLShift) & 511) - kHklOff)};
                         const float4 p0 = __ldg(packs + 3 * ubi);
                         const float4 p1 = __ldg(packs + 3 * ubi + 1);
                         const float4 p2 = __ldg(packs + 3 * ubi + 2);

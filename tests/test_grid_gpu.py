@@ -339,3 +339,26 @@ def test_g_outside_the_built_bounds(B, oracle, scene, method, cuda):
     tols = [0.05, 0.2]
     c = B.score_grid(ubis[:300], grid, tols, method=method).cpu().numpy()
     assert np.array_equal(c, oracle.score_many(ubis[:300], moved, tols))
+
+
+def test_bins_more_ubis_than_a_box_record_holds(B, oracle, scene, cuda):
+    """A box record holds its UBI's index within a range of 2^20 UBIs:
+    1,053,576 UBIs are joined in two ranges, and every UBI's counts are the
+    reference's."""
+    ps, _ = scene
+    g = ps.gv[:4000]
+    rng = np.random.default_rng(7)
+    m = (1 << 20) + 5000
+    q = rng.normal(size=(m, 4))
+    q /= np.linalg.norm(q, axis=1)[:, None]
+    a, b, c, d = q.T
+    rot = np.stack([np.stack([1 - 2 * (c * c + d * d), 2 * (b * c - a * d), 2 * (b * d + a * c)], -1),
+                    np.stack([2 * (b * c + a * d), 1 - 2 * (b * b + d * d), 2 * (c * d - a * b)], -1),
+                    np.stack([2 * (b * d - a * c), 2 * (c * d + a * b), 1 - 2 * (b * b + c * c)], -1)],
+                   1)
+    ubis = rng.uniform(0.8, 1.6, size=(m, 1, 1)) * rot    # small cells: few boxes each
+    grid = B.GvecGrid(g)
+    tols = [0.1, 0.25]
+    cnt = B.score_grid(ubis, grid, tols, method="bins").cpu().numpy()
+    assert grid.stats()["fallback_ubis"] == 0
+    assert np.array_equal(cnt, oracle.score_many(ubis, g, tols))

@@ -185,14 +185,24 @@ k_scatter(const double* __restrict__ gv, int64_t n, const Header* __restrict__ H
     }
 }
 
-// order each cell's entries by original index: the layout, and so every
-// result, does not depend on the order the scatter's atomics ran in
+// Each cell's entries ordered by original index (the layout, and so every
+// result, does not depend on the order the scatter's atomics ran in) and the
+// FP32 (round to nearest) copy of the sorted g for staging, with the g's x cell
+// (as int bits) in w.  One thread per position; the thread at a cell's first
+// position sorts the cell and writes its copies.  Threads at the cell's other
+// positions may read coordinates the sort is moving, but every value there is
+// a coordinate of a g of that cell, so they find the same cell and skip it.
 __global__ void __launch_bounds__(kGT)
-k_sort_cells(const int* __restrict__ start, int64_t ncells, double* __restrict__ gs,
-             int* __restrict__ gidx) {
-    for (int64_t c = (int64_t)blockIdx.x * kGT + threadIdx.x; c < ncells;
-         c += (int64_t)gridDim.x * kGT) {
-        const int a = start[c], b = start[c + 1];
+k_sort_cells_f32(const int* __restrict__ start, const Header* __restrict__ Hp, double* gs,
+                 int* gidx, float4* __restrict__ g4) {
+    const Header H = *Hp;
+    const int64_t nreg = start[H.ncells];
+    for (int64_t p = (int64_t)blockIdx.x * kGT + threadIdx.x; p < nreg;
+         p += (int64_t)gridDim.x * kGT) {
+        const int64_t c = cell_of(gs[3 * p], gs[3 * p + 1], gs[3 * p + 2], H);
+        const int a = start[c];
+        if (a != p) continue;
+        const int b = start[c + 1];
         for (int i = a + 1; i < b; i++) {
             const int key = gidx[i];
             const double x = gs[3 * (int64_t)i], y = gs[3 * (int64_t)i + 1],
@@ -210,21 +220,11 @@ k_sort_cells(const int* __restrict__ start, int64_t ncells, double* __restrict__
             gs[3 * (int64_t)j + 4] = y;
             gs[3 * (int64_t)j + 5] = z;
         }
+        for (int64_t q = a; q < b; q++)
+            g4[q] = make_float4(__double2float_rn(gs[3 * q]), __double2float_rn(gs[3 * q + 1]),
+                                __double2float_rn(gs[3 * q + 2]),
+                                __int_as_float(coord_x(gs[3 * q], H)));
     }
-}
-
-// FP32 (round to nearest) copy of the cell-sorted regular g, for staging,
-// with the g's x cell (as int bits) in w
-__global__ void __launch_bounds__(kGT)
-k_sorted_f32(const int* __restrict__ start, const Header* __restrict__ Hp,
-             const double* __restrict__ gs, float4* __restrict__ g4) {
-    const Header H = *Hp;
-    const int64_t nreg = start[H.ncells];
-    for (int64_t p = (int64_t)blockIdx.x * kGT + threadIdx.x; p < nreg;
-         p += (int64_t)gridDim.x * kGT)
-        g4[p] = make_float4(__double2float_rn(gs[3 * p]), __double2float_rn(gs[3 * p + 1]),
-                            __double2float_rn(gs[3 * p + 2]),
-                            __int_as_float(coord_x(gs[3 * p], H)));
 }
 
 // Per-warp queue of hkl that reach the data.  Enumeration: 32 (h, k) columns
@@ -896,11 +896,9 @@ extern "C" int id11b_dev_build_grid(const double* gv, int64_t n, float gmax, flo
         k_scatter<<<grid_for(n, kGT), kGT, 0, st>>>(gv, n, H, start, cnt, (double*)(b + L.g),
                                                     (int*)(b + L.idx), spos, (int*)(b + L.spec));
         ID11B_CHECK_LAUNCH();
-        k_sort_cells<<<grid_for(ncells, kGT), kGT, 0, st>>>(start, ncells, (double*)(b + L.g),
-                                                            (int*)(b + L.idx));
-        ID11B_CHECK_LAUNCH();
-        k_sorted_f32<<<grid_for(n, kGT), kGT, 0, st>>>(start, H, (const double*)(b + L.g),
-                                                       (float4*)(b + L.g4));
+        k_sort_cells_f32<<<grid_for(n, kGT), kGT, 0, st>>>(start, H, (double*)(b + L.g),
+                                                            (int*)(b + L.idx),
+                                                            (float4*)(b + L.g4));
         ID11B_CHECK_LAUNCH();
     }
     return ID11B_OK;

@@ -549,7 +549,8 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
     from imaged11_b200 import tune
     base = batch.GvecGrid(gv, xsub=1)
     shape, ptable = tune.tune_grid(ub_d[::10], gv, [tol],
-                                   cell_factors=(0.8, 0.9, 1.0, 1.25), xsubs=(2, 4, 8),
+                                   cell_factors=(0.8, 1.0, 1.25, 1.5, 2.0, 2.5, 3.0),
+                                   xsubs=(4, 8, 16),
                                    reps=1)
     state.update(cs=base.cs * shape[0], xsub=shape[1])
     del base

@@ -153,8 +153,8 @@ def grid_key(n):
     return "grid|%s|%d" % (_device_name(), _bucket(n))
 
 
-def tune_grid(ubis, gv, tols, cell_factors=(0.8, 0.85, 0.9, 1.0, 1.25), xsubs=(1, 2, 4, 8),
-              reps=2, method=None):
+def tune_grid(ubis, gv, tols, cell_factors=(0.8, 0.85, 0.9, 1.0, 1.25, 1.5, 2.0),
+              xsubs=(1, 2, 4, 8), reps=2, method=None):
     """Time score_grid on these inputs for cell-index shapes: y/z cell side =
     factor x the default (about one g per cell of the bounding cube) and x cut
     xsub times finer, and for its two methods; cache the fastest shape and

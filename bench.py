@@ -513,7 +513,12 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
         ev[2].record()
         d2.fill_(2.0)
         lab.fill_(-1)
-        batch.score_and_assign_grid(u_ref_d, grid, tol, d2, lab)
+        # the assignment runs the lookup: an index of the lookup's best shape
+        # when that differs from the scoring's (its build is timed here)
+        agrid = grid if shape is None or state.get("walk_shape") in (None, tuple(shape)) else \
+            batch.GvecGrid(gv, cell=state["base_cs"] * state["walk_shape"][0],
+                           xsub=state["walk_shape"][1])
+        batch.score_and_assign_grid(u_ref_d, agrid, tol, d2, lab)
         ev[3].record()
         lab_s, order = torch.sort(lab, stable=True)
         first = int((lab_s < 0).sum().item())
@@ -544,15 +549,17 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
         state.update(grid=grid, order=order, off=off, grains=grains)
 
     run([torch.cuda.Event(enable_timing=True) for _ in range(6)])   # warm-up (module loads)
-    # index shape for this peak set from the autotuner, on a tenth of the trials
-    # (untimed setup; the counts do not depend on it)
+    # index shape for this peak set from the autotuner, on all the trials (a
+    # tenth of them favours larger cells: per-row staging weighs more against
+    # fewer boxes) -- untimed setup; the counts do not depend on it
     from imaged11_b200 import tune
     base = batch.GvecGrid(gv, xsub=1)
-    shape, ptable = tune.tune_grid(ub_d[::10], gv, [tol],
-                                   cell_factors=(0.8, 1.0, 1.25, 1.5, 2.0, 2.5, 3.0),
-                                   xsubs=(4, 8, 16),
+    shape, ptable = tune.tune_grid(ub_d, gv, [tol],
+                                   cell_factors=None, xsubs=(4, 8, 16),
                                    reps=1)
-    state.update(cs=base.cs * shape[0], xsub=shape[1])
+    walk = [(t_, ms) for t_, ms in ptable if t_[2] == "walk"]
+    state.update(cs=base.cs * shape[0], xsub=shape[1], base_cs=base.cs,
+                 walk_shape=tuple(min(walk, key=lambda x: x[1])[0][:2]) if walk else None)
     del base
     # the binned join's workspace for the tuned shape, sized before the timed
     # run (untimed setup, as the workspace a caller keeps between scans)
@@ -584,7 +591,11 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
            "geometry_step": out["geometry_step"],
            "index_shape": {"cell_factor": shape[0], "xsub": shape[1],
                            "method": tune.grid_method(n),
-                           "tuning_ms_tenth_of_trials": {"%g,%d,%s" % t_: round(ms, 2)
+                           "assignment_index": None if state["walk_shape"] in
+                           (None, tuple(shape)) else
+                           {"cell_factor": state["walk_shape"][0],
+                            "xsub": state["walk_shape"][1]},
+                           "tuning_ms": {"%g,%d,%s" % t_: round(ms, 2)
                                                          for t_, ms in ptable}},
            "score_batch_fp32_ms": e0.elapsed_time(e1),
            "score_grid_counts_equal_fp32": bool(torch.equal(c32, cbuf)),

@@ -153,22 +153,60 @@ def grid_key(n):
     return "grid|%s|%d" % (_device_name(), _bucket(n))
 
 
-def tune_grid(ubis, gv, tols, cell_factors=(0.8, 0.85, 0.9, 1.0, 1.25, 1.5, 2.0),
-              xsubs=(1, 2, 4, 8), reps=2, method=None):
+def halo_cell_factor(ubis, base, tmax):
+    """The smallest y/z cell side, as a factor of base.cs, at which the binned
+    join's halo is one row of cells each way: the join stages for each row of
+    cells the g within W + 2 eps of it (W the largest widened box half width,
+    eps = 2e-5 (1 + G)), over ceil((W + 2 eps) / cs) rows each way, and a
+    second ring of rows multiplies the staging (measured: 20,000 UBIs x 1.1M g
+    took 2.78 ms just above this side and 3.16 ms just below it).  W is
+    estimated here as the enumeration widens each box: (tmax + 1e-6) times the
+    norm of UB's row plus the FP32 centre margin 4 2^-24 max|hkl| sum|UB row|,
+    over the UBIs the join takes (finite, invertible, with fewer candidate hkl
+    than g).  None if no UBI qualifies."""
+    torch = _torch()
+    u = ubis.reshape(-1, 3, 3)
+    if u.shape[0] == 0:
+        return None
+    det = torch.nan_to_num(torch.linalg.det(u).abs(), nan=0.0, posinf=0.0)
+    ok = det > 0
+    ub = torch.linalg.inv(torch.where(ok[:, None, None], u,
+                                      torch.eye(3, dtype=u.dtype, device=u.device)))
+    G = base.gmax * (1 + 1e-6)
+    hm = (u.abs().sum(dim=2) * G + 1.0).ceil()                     # |hkl| bound per row
+    ok &= (2 * hm + 1).prod(dim=1) <= base.n
+    w = (tmax + 1e-6) * ub.norm(dim=2) * (1 + 1e-9) + \
+        4 * 2.0 ** -24 * hm.max(dim=1, keepdim=True).values * ub.abs().sum(dim=2)
+    w = torch.nan_to_num(w, nan=0.0, posinf=0.0).max(dim=1).values
+    if not bool(ok.any()):
+        return None
+    W = float(torch.where(ok, w, torch.zeros_like(w)).max().item())
+    eps = 2e-5 * (1 + G)
+    return (W + 2 * eps) * (1 + 1e-3) / base.cs
+
+
+def tune_grid(ubis, gv, tols, cell_factors=None, xsubs=(1, 2, 4, 8), reps=2, method=None):
     """Time score_grid on these inputs for cell-index shapes: y/z cell side =
     factor x the default (about one g per cell of the bounding cube) and x cut
     xsub times finer, and for its two methods; cache the fastest shape and
     method per g-count bucket (GvecGrid uses the shape when built without an
     explicit one, score_grid the method when called without one) and return
-    ((factor, xsub), table of ((factor, xsub, method), ms)).  method: time
-    only that score_grid method ("bins" or "walk"; None: both, "bins" where
-    the tolerances and the shape allow it)."""
+    ((factor, xsub), table of ((factor, xsub, method), ms)).  cell_factors:
+    None tries 0.8, 1.0 and 1.25 and 1.0, 1.12, 1.25 and 1.5 times
+    halo_cell_factor (the binned join's best sides lie just above it: 0.9 x the
+    default for 20,000 UBIs x 1.1M g, 2 x for 10,000 x 10M).  method: time only
+    that score_grid method ("bins" or "walk"; None: both, "bins" where the
+    tolerances and the shape allow it)."""
     from . import batch
     torch = _torch()
     g = batch._dev(gv, torch.float64).reshape(-1, 3)
     u = batch._dev(ubis, torch.float64).reshape(-1, 9)
     base = batch.GvecGrid(g, xsub=1)
     t = batch._tols(tols)
+    if cell_factors is None:
+        f = halo_cell_factor(u, base, float(t.max()))
+        cell_factors = sorted({0.8, 1.0, 1.25} |
+                              ({round(f * k, 4) for k in (1.0, 1.12, 1.25, 1.5)} if f else set()))
     out = torch.empty((u.shape[0], len(t)), dtype=torch.int32, device=g.device)
     table = []
     for f in cell_factors:

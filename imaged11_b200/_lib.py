@@ -73,6 +73,8 @@ _SIGNATURES = [
     ("id11b_assign_workspace_bytes", _i64, [_i64]),
     ("id11b_dev_assign_grid_pass", _i, [_p, _i64, _i64, _i64, _i, _i, _p, _d, _p, _i, _p, _p,
                                          _p]),
+    ("id11b_dev_assign_grid_bins", _i, [_p, _i64, _p, _i64, _i, _i, _p, _d, _p, _p, _p, _p, _i64,
+                                        _p]),
     ("id11b_dev_assign_grid_final", _i, [_p, _i64, _p, _p, _i64, _i, _i, _p, _d, _p, _p, _p, _p,
                                           _p, _p]),
     ("id11b_dev_score_and_assign_grid", _i, [_p, _i64, _p, _p, _i64, _i, _i, _p, _d, _p, _p,

@@ -321,7 +321,8 @@ def refine_grid(ubis, grid, tol, iters=1):
     return u.view(-1, 3, 3), npk, mean
 
 
-def score_and_assign_grid(ubis, grid, tol, drlv2, labels, grain_labels=None, npk=False):
+def score_and_assign_grid(ubis, grid, tol, drlv2, labels, grain_labels=None, npk=False,
+                          method="walk", workspace=None):
     """score_and_assign (ImageD11 src/closest.c:366-397) for every grain in
     order, as ImageD11/indexing.py fight_over_peaks calls it, in one pass
     over the cell index: drlv2 (n float64) and labels (n int32) -- CUDA
@@ -329,7 +330,10 @@ def score_and_assign_grid(ubis, grid, tol, drlv2, labels, grain_labels=None, npk
     the sequential calls score_and_assign(ubis[i], gv, tol, drlv2, labels,
     grain_labels[i]).  grain_labels: strictly increasing ints (default
     0 .. m-1).  With npk=True also returns the int32 count of peaks holding
-    each grain's label at the end."""
+    each grain's label at the end.  method: "walk" looks up the g near each
+    grain's lattice points; "bins" takes the pairs from the binned join (tol
+    below 0.4, the grid within the join's limits; workspace: a BinsWorkspace
+    to reuse) -- the same result."""
     torch = _torch()
     u = _dev(ubis, torch.float64).reshape(-1, 9)
     m = u.shape[0]
@@ -359,6 +363,33 @@ def score_and_assign_grid(ubis, grid, tol, drlv2, labels, grain_labels=None, npk
             raise ValueError("grain_labels must be strictly increasing")
         gl = gl.contiguous()
     counts = torch.empty(m, dtype=torch.int32, device=dev) if npk else None
+    if method == "bins":
+        if not (float(tol) < BINS_TOL_LIMIT and bins_fit(grid)):
+            raise ValueError("method='bins' needs tol < %g and a grid within the join's "
+                             "limits" % BINS_TOL_LIMIT)
+        boxes = bins_box_estimate(u, grid, float(tol))
+        bws = workspace if workspace is not None and workspace.fits(m, grid, boxes) else \
+            BinsWorkspace(m, grid, boxes)
+        best = torch.empty(grid.n, dtype=torch.int64, device=dev)
+        win = torch.empty(grid.n, dtype=torch.int32, device=dev)
+        args = (u.data_ptr(), m)
+        shape = (grid.n, grid.nx, grid.xsub, grid.buf.data_ptr(), float(tol))
+        check(lib.id11b_dev_assign_grid_pass(*args, 0, *shape, d.data_ptr(), -1, best.data_ptr(),
+                                             win.data_ptr(), _stream()), "assign_pass")
+        check(lib.id11b_dev_assign_grid_bins(*args, grid.gv.data_ptr(), *shape, d.data_ptr(),
+                                             best.data_ptr(), win.data_ptr(), bws.buf.data_ptr(),
+                                             bws.buf.numel(), _stream()), "assign_grid_bins")
+        check(lib.id11b_dev_assign_grid_final(*args, gl.data_ptr() if gl is not None else None,
+                                              grid.gv.data_ptr(), *shape, best.data_ptr(),
+                                              win.data_ptr(), d.data_ptr(), lab.data_ptr(),
+                                              counts.data_ptr() if npk else None, _stream()),
+              "assign_final")
+        if host:
+            drlv2[:] = d.cpu().numpy()
+            labels[:] = lab.cpu().numpy()
+        return counts
+    if method != "walk":
+        raise ValueError("method: 'walk' or 'bins'")
     ws = torch.empty(lib.id11b_assign_workspace_bytes(grid.n), dtype=torch.uint8, device=dev)
     check(lib.id11b_dev_score_and_assign_grid(u.data_ptr(), m,
                                               gl.data_ptr() if gl is not None else None,

@@ -133,6 +133,12 @@ struct JoinParams {
     float rlo, rhi, cs;
     int R, Rx, nx, nxx;
     int64_t i0;                    // first UBI of the range (box records are relative to it)
+    // assignment (k_join's AS modes): sorted position -> g index, each g's
+    // drlv2 on entry, the smallest drlv2 bits and the lowest grain reaching it
+    const int* gidx;
+    const double* d0;
+    unsigned long long* best;
+    int* lab;
 };
 
 // box record (64 bits): UBI (kUbiBits, relative to the range) | h + 256 (9) |
@@ -493,13 +499,29 @@ __device__ __noinline__ Exact exact_pair(const double* __restrict__ ubis, int64_
 // A pair inside a band (or, with sums, any pair below hmax), evaluated
 // exactly: counted for the tolerances its FP64 drlv2 clears under its own hkl
 // (those it cleared in FP32 by more than the band were counted already).
-template <int NT, bool SUMS>
+//
+// AS 1 and 2 (assignment, NT 1, SUMS): the two passes of k_assign
+// (gvec_grid.cu) on the pair -- below tol^2 and below the g's drlv2 on entry,
+// pass 1 takes the smallest drlv2 bits per g, pass 2 the lowest UBI index
+// reaching them.
+template <int NT, bool SUMS, int AS>
 __device__ __forceinline__ void rare_pair(float s, int pos, const JoinParams& P,
                                           const double* __restrict__ ubis, int64_t ubi,
                                           const double* __restrict__ gs, const float* hkf,
                                           int cnt[NT], unsigned long long sum[NT]) {
     const Exact e = exact_pair(ubis, ubi, gs, pos, hkf[0], hkf[1], hkf[2]);
     if (!e.own) return;
+    if (AS) {
+        if (!(e.s < P.t2[0])) return;
+        const int k = __ldg(P.gidx + pos);
+        if (!(e.s < __ldg(P.d0 + k))) return;
+        const unsigned long long b = (unsigned long long)__double_as_longlong(e.s);
+        if (AS == 1)
+            atomicMin(P.best + k, b);
+        else if (P.best[k] == b)
+            atomicMin(P.lab + k, (int)ubi);
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < NT; j++) {
         if (!(e.s < P.t2[j])) continue;
@@ -529,7 +551,7 @@ struct Staged {  // the tile of staged g, structure of arrays (pairs read as 64 
 // not above it -- one select chain and one compare instead of a test per
 // tolerance.  (If s lies in band i <= J, J the largest j with lo_j <= s, then
 // s < hi_i <= hi_J.)
-template <int NT, bool SUMS, bool RANKED>
+template <int NT, bool SUMS, bool RANKED, int AS>
 __device__ __forceinline__ void test_range(const Staged& t, int ga, int gb, const uint64_t uu[9],
                                            const uint64_t hh[3], const float* hkf,
                                            const JoinParams& P, const double* __restrict__ ubis,
@@ -585,8 +607,8 @@ __device__ __forceinline__ void test_range(const Staged& t, int ga, int gb, cons
         }
         if (ra || rb) {
             ntest += (unsigned)ra + (unsigned)rb;
-            if (ra) rare_pair<NT, SUMS>(sa, t.pos[q], P, ubis, ubi, gs, hkf, cnt, sum);
-            if (rb) rare_pair<NT, SUMS>(sb, t.pos[q + 1], P, ubis, ubi, gs, hkf, cnt, sum);
+            if (ra) rare_pair<NT, SUMS, AS>(sa, t.pos[q], P, ubis, ubi, gs, hkf, cnt, sum);
+            if (rb) rare_pair<NT, SUMS, AS>(sb, t.pos[q + 1], P, ubis, ubi, gs, hkf, cnt, sum);
         }
     }
 }
@@ -621,7 +643,7 @@ __device__ __forceinline__ void block_scan(const int* a, int* b, int len, int* s
 // tiles of at most kGMax, each sorted by x cell, and every run of 32 sorted
 // boxes (one warp) is tested against the staged g in the x cells its boxes
 // can reach.
-template <int NT, bool SUMS, bool RANKED>
+template <int NT, bool SUMS, bool RANKED, int AS = 0>
 __global__ void __launch_bounds__(kJT, kJoinMinBlocks)
 k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nrows,
        int nhalo, BinInfo* __restrict__ info, const float4* __restrict__ packs,
@@ -816,10 +838,10 @@ k_join(const uint64_t* __restrict__ recs, const int* __restrict__ rstart, int nr
                             cnt[j] = 0;
                             sum[j] = 0ull;
                         }
-                        test_range<NT, SUMS, RANKED>(T, ga, gb, uu, hh, hkf, P, ubis, ubi, gs,
-                                                     cnt, sum, ntest);
+                        test_range<NT, SUMS, RANKED, AS>(T, ga, gb, uu, hh, hkf, P, ubis, ubi,
+                                                         gs, cnt, sum, ntest);
 #pragma unroll
-                        for (int j = 0; j < NT; j++) {
+                        for (int j = 0; j < NT && !AS; j++) {
                             if (cnt[j]) atomicAdd(counts + ubi * NT + P.ord[j], cnt[j]);
                             if (SUMS && sum[j])
                                 atomicAdd(reinterpret_cast<unsigned long long*>(
@@ -924,15 +946,50 @@ k_special(const double* __restrict__ ubis, int64_t m, const double* __restrict__
     }
 }
 
-template <int NT, bool SUMS, bool RANKED>
+// The assignment's rules (k_assign, gvec_grid.cu) for the UBIs outside the
+// binned path's limits: exact FP64 over every regular g, one warp per
+// (listed UBI, part); PASS 0 the smallest drlv2 bits, PASS 1 the lowest UBI.
+template <int PASS>
+__global__ void __launch_bounds__(kBT)
+k_assign_fallback(const double* __restrict__ ubis, const int* __restrict__ list, int nlist,
+                  const Header* __restrict__ Hp, const int* __restrict__ start,
+                  const double* __restrict__ gs, const int* __restrict__ gidx, double tol,
+                  const double* __restrict__ d0, unsigned long long* __restrict__ best,
+                  int* __restrict__ lab) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wk = ((int64_t)blockIdx.x * kBT + threadIdx.x) >> 5;
+    if (wk >= (int64_t)nlist * kFallbackParts) return;  // uniform per warp
+    const int i = list[wk / kFallbackParts];
+    const int part = (int)(wk % kFallbackParts);
+    const int64_t nreg = start[Hp->ncells];
+    const double t2 = tol * tol;
+    double u[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) u[e] = ubis[9 * (int64_t)i + e];
+    for (int64_t f = (int64_t)part * 32 + lane; f < nreg; f += 32 * (int64_t)kFallbackParts) {
+        double ih[3];
+        const double s = drlv2_exact(u, gs[3 * f], gs[3 * f + 1], gs[3 * f + 2], ih);
+        if (!(s < t2)) continue;
+        const int k = gidx[f];
+        if (!(s < d0[k])) continue;
+        const unsigned long long b = (unsigned long long)__double_as_longlong(s);
+        if (PASS == 0)
+            atomicMin(best + k, b);
+        else if (best[k] == b)
+            atomicMin(lab + k, i);
+    }
+}
+
+template <int NT, bool SUMS, bool RANKED, int AS = 0>
 int launch_join_k(int grid, size_t smem, const uint64_t* recs, const int* rstart, int nrows,
                   int nhalo, BinInfo* info, const float4* packs, const double* ubis, Header* H,
                   const int* start, const double* gs, const float4* g4, const JoinParams& P,
                   int* counts, double* sums, cudaStream_t st) {
-    ID11B_CHECK(cudaFuncSetAttribute(k_join<NT, SUMS, RANKED>,
+    ID11B_CHECK(cudaFuncSetAttribute(k_join<NT, SUMS, RANKED, AS>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_join<NT, SUMS, RANKED><<<grid, kJT, smem, st>>>(recs, rstart, nrows, nhalo, info, packs,
-                                                      ubis, H, start, gs, g4, P, counts, sums);
+    k_join<NT, SUMS, RANKED, AS><<<grid, kJT, smem, st>>>(recs, rstart, nrows, nhalo, info, packs,
+                                                          ubis, H, start, gs, g4, P, counts,
+                                                          sums);
     ID11B_CHECK_LAUNCH();
     return ID11B_OK;
 }
@@ -1039,25 +1096,35 @@ extern "C" int64_t id11b_grid_bins_workspace_bytes(int64_t m, int32_t nx, int32_
              : ntol == 3 ? FN<3, false>(__VA_ARGS__)                                        \
                          : FN<4, false>(__VA_ARGS__)))
 
-extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const double* gv,
-                                         int64_t n, int32_t nx, int32_t xsub,
-                                         const void* gridbuf, const double* tols_host, int ntol,
-                                         int32_t* counts, double* sums, void* ws,
-                                         int64_t ws_bytes, void* stream) {
-    if (!tols_host || ntol < 1 || ntol > ID11B_MAX_TOLS || m < 0 || n < 0 ||
-        !grid_dims_ok(nx, xsub) || !gridbuf || !ws || (m > 0 && (!ubis || !counts)) ||
-        (n > 0 && !gv))
-        return ID11B_ERR_ARG;
-    Tols T;
-    double tmax = 0.;
-    for (int j = 0; j < ID11B_MAX_TOLS; j++) T.t[j] = j < ntol ? tols_host[j] : 0.;
-    for (int j = 0; j < ntol; j++) {
-        if (!(tols_host[j] >= 0.) || !(tols_host[j] < kTolLimit)) return ID11B_ERR_ARG;
-        tmax = fmax(tmax, tols_host[j]);
-    }
-    T.fix = id11b::fixsum_scale(n, tmax);
-    if (((uintptr_t)gridbuf & 255) || ((uintptr_t)ws & 255)) return ID11B_ERR_ALIGN;
-    if (m > INT32_MAX - 1) return ID11B_ERR_SIZE;
+// What a join launch of the binned pipeline needs (one range of UBIs).
+struct JoinLaunch {
+    int grid;
+    size_t smem;
+    bool ranked;
+    const uint64_t* recs;
+    const int* rstart;
+    int nrows, nhalo;
+    BinInfo* info;
+    const float4* packs;
+    Header* H;
+    const int* start;
+    const double* gs;
+    const float4* g4;
+    const JoinParams* P;
+};
+
+// The binned pipeline shared by scoring and assignment: the counting
+// enumeration, the UBI ranges that fit the workspace, the join's band and
+// region; then for each pass, for each range, the box records (written again
+// only when there are several ranges) and join(pass, launch), and after the
+// ranges after(pass, fallback list, its length, g outside the regular range,
+// ...).  ctas(smem, ranked): resident join CTAs per SM.  P.fix is T.fix; the
+// assignment's fields of P are set by the caller's P0.
+template <class Ctas, class Join, class After>
+static int bins_pipeline(const double* ubis, int64_t m, int64_t n, int32_t nx, int32_t xsub,
+                         const void* gridbuf, const Tols& T, int ntol, double tmax, void* ws,
+                         int64_t ws_bytes, cudaStream_t st, int passes, const JoinParams& P0,
+                         Ctas ctas, Join join, After after) {
     const int nrows = nx * nx;
     const int nxx = nx * xsub;
     const int nblk = (nrows + kRowBlock - 1) / kRowBlock;
@@ -1069,7 +1136,6 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     while (cap > 0 && (int64_t)bin_layout(m, nrows, cap).bytes > ws_bytes) cap -= 1 + cap / 1024;
     if (cap > INT32_MAX - 1) cap = INT32_MAX - 1;
     const BinLayout B = bin_layout(m, nrows, cap);
-    cudaStream_t st = (cudaStream_t)stream;
     const Layout L = layout(n, (int64_t)nrows * nxx);
     char* g = (char*)gridbuf;
     Header* H = (Header*)g;
@@ -1090,8 +1156,6 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     uint64_t* recs = (uint64_t*)(w + B.recs);
     ID11B_CHECK(cudaMemsetAsync(&H->nfallback, 0, 3 * sizeof(unsigned long long), st));
     if (m == 0) return ID11B_OK;
-    ID11B_CHECK(cudaMemsetAsync(counts, 0, sizeof(int32_t) * (size_t)(m * ntol), st));
-    if (sums) ID11B_CHECK(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)(m * ntol), st));
     ID11B_CHECK(cudaMemsetAsync(info, 0, sizeof(BinInfo), st));
     // the enumeration's CTAs (same count and UBI ranges in both passes)
     static thread_local int enum_per_sm = 0;
@@ -1136,7 +1200,7 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     cuts.push_back(m);
     // the screening kernel's band (score_batch.cu) for gmax = G and the largest
     // row sum of the binned UBIs; the region geometry
-    JoinParams P;
+    JoinParams P = P0;
     P.fix = T.fix;
     bool ranked = false;
     {
@@ -1188,45 +1252,150 @@ extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const do
     const size_t jsmem = sizeof(uint64_t) * kBMax + 4 * sizeof(float) * kGMax +
                          4 * sizeof(int) * (size_t)(std::max(nxx, nhalo) + 1) +
                          2 * sizeof(int) * (size_t)(nhalo + 1);
-    const int jgrid = num_sms() * ID11B_BINS_DISPATCH(join_ctas, jsmem, ranked);
+    const int jgrid = num_sms() * ctas(jsmem, ranked);
     cudaEvent_t ev0 = t_join_start, ev1 = t_join_stop;
     t_join_start = t_join_stop = nullptr;
     bool ev0_done = false;
-    for (size_t c = 0; c + 1 < cuts.size() && bi.total > 0; c++) {
-        const int64_t i0 = cuts[c], mc = cuts[c + 1] - cuts[c];
-        if (cuts.size() > 2) {
-            egrid = enumerate(0, i0, mc, 0);
-            ID11B_CHECK_LAUNCH();
+    for (int pass = 0; pass < passes; pass++) {
+        for (size_t c = 0; c + 1 < cuts.size() && bi.total > 0; c++) {
+            const int64_t i0 = cuts[c], mc = cuts[c + 1] - cuts[c];
+            // one range keeps its records from pass to pass
+            if (pass == 0 || cuts.size() > 2) {
+                if (cuts.size() > 2) {
+                    egrid = enumerate(0, i0, mc, 0);
+                    ID11B_CHECK_LAUNCH();
+                }
+                k_blk_offsets<<<grid_for((int64_t)nblk * 32, kGT), kGT, 0, st>>>(cta_blk, egrid,
+                                                                                nblk, blktot);
+                ID11B_CHECK_LAUNCH();
+                ID11B_CHECK(cudaMemsetAsync(blktot + nblk, 0, sizeof(int), st));
+                int rc = scan(blktot, nblk + 1, blkstart, tot, st);
+                if (rc) return rc;
+                enumerate(1, i0, mc, 0);
+                ID11B_CHECK_LAUNCH();
+                k_rowsplit<<<(unsigned)std::min(nblk, num_sms() * kRSPerSM), kRS, 0, st>>>(
+                    tmp, blkstart, nblk, nrows, rstart, recs);
+                ID11B_CHECK_LAUNCH();
+            }
+            ID11B_CHECK(cudaMemsetAsync(&info->next_row, 0, sizeof(int), st));
+            P.i0 = i0;
+            if (ev0 && !ev0_done) {
+                ID11B_CHECK(cudaEventRecord(ev0, st));
+                ev0_done = true;
+            }
+            const int rc = join(pass, JoinLaunch{jgrid, jsmem, ranked, recs, rstart, nrows, nhalo,
+                                                 info, packs, H, start, gs, g4, &P});
+            if (rc) return rc;
         }
-        k_blk_offsets<<<grid_for((int64_t)nblk * 32, kGT), kGT, 0, st>>>(cta_blk, egrid, nblk,
-                                                                        blktot);
-        ID11B_CHECK_LAUNCH();
-        ID11B_CHECK(cudaMemsetAsync(blktot + nblk, 0, sizeof(int), st));
-        int rc = scan(blktot, nblk + 1, blkstart, tot, st);
-        if (rc) return rc;
-        enumerate(1, i0, mc, 0);
-        ID11B_CHECK_LAUNCH();
-        k_rowsplit<<<(unsigned)std::min(nblk, num_sms() * kRSPerSM), kRS, 0, st>>>(
-            tmp, blkstart, nblk, nrows, rstart, recs);
-        ID11B_CHECK_LAUNCH();
-        ID11B_CHECK(cudaMemsetAsync(&info->next_row, 0, sizeof(int), st));
-        P.i0 = i0;
-        if (ev0 && !ev0_done) {
-            ID11B_CHECK(cudaEventRecord(ev0, st));
-            ev0_done = true;
+        if (ev1 && pass == passes - 1) {
+            if (!ev0_done) ID11B_CHECK(cudaEventRecord(ev0, st));
+            ID11B_CHECK(cudaEventRecord(ev1, st));
         }
-        rc = ID11B_BINS_DISPATCH(launch_join, jgrid, jsmem, ranked, recs, rstart, nrows, nhalo,
-                                 info, packs, ubis, H, start, gs, g4, P, counts, sums, st);
+        const int rc = after(pass, fallback, (int)bi.nfallback, nspecial, H, start, gs,
+                             (const int*)(g + L.spec), (const int*)(g + L.spos) + n);
         if (rc) return rc;
     }
-    if (ev1) {
-        if (!ev0_done) ID11B_CHECK(cudaEventRecord(ev0, st));
-        ID11B_CHECK(cudaEventRecord(ev1, st));
+    return ID11B_OK;
+}
+
+extern "C" int id11b_dev_score_grid_bins(const double* ubis, int64_t m, const double* gv,
+                                         int64_t n, int32_t nx, int32_t xsub,
+                                         const void* gridbuf, const double* tols_host, int ntol,
+                                         int32_t* counts, double* sums, void* ws,
+                                         int64_t ws_bytes, void* stream) {
+    if (!tols_host || ntol < 1 || ntol > ID11B_MAX_TOLS || m < 0 || n < 0 ||
+        !grid_dims_ok(nx, xsub) || !gridbuf || !ws || (m > 0 && (!ubis || !counts)) ||
+        (n > 0 && !gv))
+        return ID11B_ERR_ARG;
+    Tols T;
+    double tmax = 0.;
+    for (int j = 0; j < ID11B_MAX_TOLS; j++) T.t[j] = j < ntol ? tols_host[j] : 0.;
+    for (int j = 0; j < ntol; j++) {
+        if (!(tols_host[j] >= 0.) || !(tols_host[j] < kTolLimit)) return ID11B_ERR_ARG;
+        tmax = fmax(tmax, tols_host[j]);
     }
-    const int rc = ID11B_BINS_DISPATCH(launch_rest, ubis, m, fallback, bi.nfallback, H, start,
-                                       gs, gv, (const int*)(g + L.spec),
-                                       (const int*)(g + L.spos) + n, nspecial > 0, T, counts,
-                                       sums, st);
+    T.fix = id11b::fixsum_scale(n, tmax);
+    if (((uintptr_t)gridbuf & 255) || ((uintptr_t)ws & 255)) return ID11B_ERR_ALIGN;
+    if (m > INT32_MAX - 1) return ID11B_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (m > 0) {
+        ID11B_CHECK(cudaMemsetAsync(counts, 0, sizeof(int32_t) * (size_t)(m * ntol), st));
+        if (sums) ID11B_CHECK(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)(m * ntol), st));
+    }
+    JoinParams P0 = {};
+    const int rc = bins_pipeline(
+        ubis, m, n, nx, xsub, gridbuf, T, ntol, tmax, ws, ws_bytes, st, 1, P0,
+        [&](size_t smem, bool ranked) { return ID11B_BINS_DISPATCH(join_ctas, smem, ranked); },
+        [&](int, const JoinLaunch& J) {
+            return ID11B_BINS_DISPATCH(launch_join, J.grid, J.smem, J.ranked, J.recs, J.rstart,
+                                       J.nrows, J.nhalo, J.info, J.packs, ubis, J.H, J.start,
+                                       J.gs, J.g4, *J.P, counts, sums, st);
+        },
+        [&](int, const int* fallback, int nfallback, int nspecial, Header* H, const int* start,
+            const double* gs, const int* special, const int* nspec) {
+            return ID11B_BINS_DISPATCH(launch_rest, ubis, m, fallback, nfallback, H, start, gs,
+                                       gv, special, nspec, nspecial > 0, T, counts, sums, st);
+        });
     if (rc) return rc;
+    if (m == 0) return ID11B_OK;
     return id11b_fixsum_finish(sums, m * ntol, T.fix, st);
+}
+
+// Both passes of the batched assignment (id11b_dev_assign_grid_pass 0 and 1
+// over all m grains) through the binned join.  best and lab as pass -1 leaves
+// them; apply id11b_dev_assign_grid_final afterwards (winners, resets and the
+// g outside the regular range).  Every (grain, g) pair the FP32 screen cannot
+// exclude from tol^2 is evaluated in the reference's FP64 arithmetic under
+// the g's own rounded hkl, so best and lab end as the lookup passes leave them.
+extern "C" int id11b_dev_assign_grid_bins(const double* ubis, int64_t m, const double* gv,
+                                          int64_t n, int32_t nx, int32_t xsub,
+                                          const void* gridbuf, double tol, const double* drlv2,
+                                          uint64_t* best, int32_t* lab, void* ws,
+                                          int64_t ws_bytes, void* stream) {
+    if (m < 0 || n < 0 || !grid_dims_ok(nx, xsub) || !gridbuf || !ws || !best || !lab ||
+        (m > 0 && !ubis) || (n > 0 && (!gv || !drlv2)) || !(tol >= 0.) || !(tol < kTolLimit))
+        return ID11B_ERR_ARG;
+    if (((uintptr_t)gridbuf & 255) || ((uintptr_t)ws & 255)) return ID11B_ERR_ALIGN;
+    if (m > INT32_MAX - 1) return ID11B_ERR_SIZE;
+    if (m == 0 || n == 0) return ID11B_OK;
+    Tols T;
+    for (int j = 0; j < ID11B_MAX_TOLS; j++) T.t[j] = j == 0 ? tol : 0.;
+    T.fix = 0.;
+    cudaStream_t st = (cudaStream_t)stream;
+    const Layout L = layout(n, (int64_t)nx * nx * nx * xsub);
+    const int* gidx = (const int*)((const char*)gridbuf + L.idx);
+    unsigned long long* bst = (unsigned long long*)best;
+    JoinParams P0 = {};
+    P0.gidx = gidx;
+    P0.d0 = drlv2;
+    P0.best = bst;
+    P0.lab = lab;
+    return bins_pipeline(
+        ubis, m, n, nx, xsub, gridbuf, T, 1, tol, ws, ws_bytes, st, 2, P0,
+        [&](size_t smem, bool) { return ctas_per_sm(k_join<1, true, false, 1>, kJT, smem); },
+        [&](int pass, const JoinLaunch& J) {
+            if (pass == 0)
+                return launch_join_k<1, true, false, 1>(J.grid, J.smem, J.recs, J.rstart, J.nrows,
+                                                        J.nhalo, J.info, J.packs, ubis, J.H,
+                                                        J.start, J.gs, J.g4, *J.P, nullptr,
+                                                        nullptr, st);
+            return launch_join_k<1, true, false, 2>(J.grid, J.smem, J.recs, J.rstart, J.nrows,
+                                                    J.nhalo, J.info, J.packs, ubis, J.H, J.start,
+                                                    J.gs, J.g4, *J.P, nullptr, nullptr, st);
+        },
+        [&](int pass, const int* fallback, int nfallback, int, Header* H, const int* start,
+            const double* gs, const int*, const int*) {
+            if (nfallback > 0) {
+                const int64_t warps = (int64_t)nfallback * kFallbackParts;
+                const unsigned blocks = (unsigned)((warps + kBW - 1) / kBW);
+                if (pass == 0)
+                    k_assign_fallback<0><<<blocks, kBT, 0, st>>>(
+                        ubis, fallback, nfallback, H, start, gs, gidx, tol, drlv2, bst, lab);
+                else
+                    k_assign_fallback<1><<<blocks, kBT, 0, st>>>(
+                        ubis, fallback, nfallback, H, start, gs, gidx, tol, drlv2, bst, lab);
+                ID11B_CHECK_LAUNCH();
+            }
+            return ID11B_OK;
+        });
 }

@@ -315,6 +315,17 @@ int id11b_dev_assign_grid_pass(const double *ubis, int64_t m, int64_t index_base
                                int32_t nx, int32_t xsub, const void *gridbuf, double tol,
                                const double *drlv2, int pass, uint64_t *best, int32_t *lab,
                                void *stream);
+/* Passes 0 and 1 of id11b_dev_assign_grid_pass for all m grains at once
+ * (index_base 0) through the binned join of id11b_dev_score_grid_bins (ws of
+ * id11b_grid_bins_workspace_bytes; tol < 0.4; the grid within the join's row
+ * and x-cell limits): best and lab as pass -1 leaves them, then
+ * id11b_dev_assign_grid_final.  Every pair the FP32 screen cannot exclude
+ * from tol^2 is evaluated in the reference's FP64 arithmetic, so best and lab
+ * end as the lookup passes leave them. */
+int id11b_dev_assign_grid_bins(const double *ubis, int64_t m, const double *gv, int64_t n,
+                               int32_t nx, int32_t xsub, const void *gridbuf, double tol,
+                               const double *drlv2, uint64_t *best, int32_t *lab, void *ws,
+                               int64_t ws_bytes, void *stream);
 int id11b_dev_assign_grid_final(const double *ubis, int64_t m, const int32_t *grain_labels,
                                 const double *gv, int64_t n, int32_t nx, int32_t xsub,
                                 const void *gridbuf, double tol, const uint64_t *best,

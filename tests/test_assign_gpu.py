@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+METHODS = ["walk", "bins"]   # the lookup and the binned join
 
 
 def sequential(oracle, ubis, gv, tol, drlv2, labels, grain_labels):
@@ -27,8 +28,9 @@ def scene():
     return ps, ubis
 
 
+@pytest.mark.parametrize("method", METHODS)
 @pytest.mark.parametrize("tol", [0.02, 0.1, 0.3])
-def test_fight_over_peaks(scene, oracle, tol, cuda):
+def test_fight_over_peaks(scene, oracle, tol, method, cuda):
     from imaged11_b200 import batch
     ps, ubis = scene
     n = len(ps.gv)
@@ -36,14 +38,16 @@ def test_fight_over_peaks(scene, oracle, tol, cuda):
     l0 = np.zeros(n, np.int32) - 1
     ref_d, ref_l = sequential(oracle, ubis, ps.gv, tol, d0, l0, range(len(ubis)))
     d, lab = d0.copy(), l0.copy()
-    npk = batch.score_and_assign_grid(ubis, batch.GvecGrid(ps.gv), tol, d, lab, npk=True)
+    npk = batch.score_and_assign_grid(ubis, batch.GvecGrid(ps.gv), tol, d, lab, npk=True,
+                                      method=method)
     assert np.array_equal(lab, ref_l)
     assert np.array_equal(d, ref_d)
     hist = np.bincount(ref_l[ref_l >= 0], minlength=len(ubis))
     assert np.array_equal(npk.cpu().numpy(), hist)
 
 
-def test_ties_labels_and_resets(scene, oracle, cuda):
+@pytest.mark.parametrize("method", METHODS)
+def test_ties_labels_and_resets(scene, oracle, method, cuda):
     from imaged11_b200 import batch
     ps, ubis = scene
     u = ubis[:60].copy()
@@ -58,12 +62,14 @@ def test_ties_labels_and_resets(scene, oracle, cuda):
     l0 = rng.choice(np.concatenate([gl, [-1, 3, 99999]]), n).astype(np.int32)
     ref_d, ref_l = sequential(oracle, u, ps.gv, 0.08, d0, l0, gl)
     d, lab = d0.copy(), l0.copy()
-    batch.score_and_assign_grid(u, batch.GvecGrid(ps.gv), 0.08, d, lab, grain_labels=gl)
+    batch.score_and_assign_grid(u, batch.GvecGrid(ps.gv), 0.08, d, lab, grain_labels=gl,
+                                method=method)
     assert np.array_equal(lab, ref_l)
     assert np.array_equal(d, ref_d)
 
 
-def test_special_g_and_device_tensors(golden, oracle, cuda):
+@pytest.mark.parametrize("method", METHODS)
+def test_special_g_and_device_tensors(golden, oracle, method, cuda):
     import torch
     from imaged11_b200 import batch
     dd = golden["scoring"]
@@ -75,7 +81,7 @@ def test_special_g_and_device_tensors(golden, oracle, cuda):
     ref_d, ref_l = sequential(oracle, ubis, gv, 0.1, d0, l0, range(len(ubis)))
     d = torch.tensor(d0, device="cuda")
     lab = torch.tensor(l0, device="cuda")
-    batch.score_and_assign_grid(ubis, batch.GvecGrid(gv), 0.1, d, lab)
+    batch.score_and_assign_grid(ubis, batch.GvecGrid(gv), 0.1, d, lab, method=method)
     assert np.array_equal(lab.cpu().numpy(), ref_l)
     assert np.array_equal(d.cpu().numpy(), ref_d, equal_nan=True)
 
@@ -119,7 +125,8 @@ def test_sharded_passes_on_one_gpu(scene, oracle, cuda):
         dist.destroy_process_group()
 
 
-def test_random_sweep(oracle, cuda):
+@pytest.mark.parametrize("method", METHODS)
+def test_random_sweep(oracle, method, cuda):
     from imaged11_b200 import batch
     rng = np.random.default_rng(79)
     for trial in range(10):
@@ -138,6 +145,6 @@ def test_random_sweep(oracle, cuda):
         for i, u in enumerate(ubis):
             _, d, lab = oracle.score_and_assign(u, gv, tol, d, lab, i)
         dd, ll = d0.copy(), l0.copy()
-        batch.score_and_assign_grid(ubis, batch.GvecGrid(gv), tol, dd, ll)
+        batch.score_and_assign_grid(ubis, batch.GvecGrid(gv), tol, dd, ll, method=method)
         assert np.array_equal(ll, lab), trial
         assert np.array_equal(dd, d), trial

@@ -513,12 +513,17 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
         ev[2].record()
         d2.fill_(2.0)
         lab.fill_(-1)
-        # the assignment runs the lookup: an index of the lookup's best shape
-        # when that differs from the scoring's (its build is timed here)
-        agrid = grid if shape is None or state.get("walk_shape") in (None, tuple(shape)) else \
-            batch.GvecGrid(gv, cell=state["base_cs"] * state["walk_shape"][0],
-                           xsub=state["walk_shape"][1])
-        batch.score_and_assign_grid(u_ref_d, agrid, tol, d2, lab)
+        if state.get("assign_bins"):
+            # the binned join on the scoring's index
+            batch.score_and_assign_grid(u_ref_d, grid, tol, d2, lab, method="bins",
+                                        workspace=state["aws"])
+        else:
+            # the lookup, on an index of the lookup's best shape when that
+            # differs from the scoring's (its build is timed here)
+            agrid = grid if shape is None or state.get("walk_shape") in (None, tuple(shape)) \
+                else batch.GvecGrid(gv, cell=state["base_cs"] * state["walk_shape"][0],
+                                    xsub=state["walk_shape"][1])
+            batch.score_and_assign_grid(u_ref_d, agrid, tol, d2, lab)
         ev[3].record()
         lab_s, order = torch.sort(lab, stable=True)
         first = int((lab_s < 0).sum().item())
@@ -566,6 +571,31 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
     g_t = batch.GvecGrid(gv, cell=state["cs"], xsub=state["xsub"])
     state["boxes"] = batch.bins_box_estimate(ub_d, g_t, tol)
     state["ws"] = batch.BinsWorkspace(len(trials), g_t, state["boxes"])
+    # the assignment's method, each timed twice on the grains (untimed setup):
+    # the binned join on this index, or the lookup on an index of its own shape
+    amodes = {}
+    if tol < batch.BINS_TOL_LIMIT and batch.bins_fit(g_t):
+        state["aws"] = batch.BinsWorkspace(ng, g_t, batch.bins_box_estimate(u_ref_d, g_t, tol))
+        amodes["bins"] = lambda: batch.score_and_assign_grid(u_ref_d, g_t, tol, d2, lab,
+                                                             method="bins",
+                                                             workspace=state["aws"])
+    if state["walk_shape"] is not None:
+        g_w = batch.GvecGrid(gv, cell=state["base_cs"] * state["walk_shape"][0],
+                             xsub=state["walk_shape"][1])
+        amodes["walk"] = lambda: batch.score_and_assign_grid(u_ref_d, g_w, tol, d2, lab)
+    amode_ms = {}
+    for k_, fn in amodes.items():
+        for _ in range(2):
+            d2.fill_(2.0)
+            lab.fill_(-1)
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record()
+            fn()
+            a1.record()
+            a1.synchronize()
+        amode_ms[k_] = a0.elapsed_time(a1)
+    state["assign_bins"] = bool(amode_ms) and min(amode_ms, key=amode_ms.get) == "bins"
+    amodes.clear()
     del g_t
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
     run(ev, shape)
@@ -591,10 +621,12 @@ def pipeline_measure(torch, dev, n_ubi=100_000, tol=0.05, rounds=5, cpu=True):
            "geometry_step": out["geometry_step"],
            "index_shape": {"cell_factor": shape[0], "xsub": shape[1],
                            "method": tune.grid_method(n),
-                           "assignment_index": None if state["walk_shape"] in
-                           (None, tuple(shape)) else
-                           {"cell_factor": state["walk_shape"][0],
-                            "xsub": state["walk_shape"][1]},
+                           "assignment": {
+                               "method": "bins" if state["assign_bins"] else "walk",
+                               "ms_untimed_trial": amode_ms,
+                               "walk_index": None if state["walk_shape"] is None else
+                               {"cell_factor": state["walk_shape"][0],
+                                "xsub": state["walk_shape"][1]}},
                            "tuning_ms": {"%g,%d,%s" % t_: round(ms, 2)
                                                          for t_, ms in ptable}},
            "score_batch_fp32_ms": e0.elapsed_time(e1),

@@ -1120,15 +1120,19 @@ def run_ours(args, rank, world, local_rank):
     egrid = [batch.GvecGrid(gbuf[j], cell=grid.cs, xsub=grid.xsub) for j in range(2)]
     assert all(eg.gv.data_ptr() == gbuf[j].data_ptr() for j, eg in enumerate(egrid))
 
+    cbuf_h = [torch.empty((m, T), dtype=torch.int32).pin_memory() for _ in range(2)]
+
     def e2e_pipelined(k):
         up = [torch.cuda.Event() for _ in range(2)]
+        done = [torch.cuda.Event() for _ in range(2)]
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
 
         def upload(j):
-            # buffer j % 2 was last read by step j - 2, which ended with a
-            # host read of its counts
+            # buffers j % 2 were last read by step j - 2: wait for its end
             with torch.cuda.stream(copy_st):
+                if j >= 2:
+                    copy_st.wait_event(done[j % 2])
                 gbuf[j % 2].copy_(gv_h, non_blocking=True)
                 ubuf[j % 2].copy_(ub_h, non_blocking=True)
                 up[j % 2].record(copy_st)
@@ -1142,14 +1146,21 @@ def run_ours(args, rank, world, local_rank):
             flush()
             main.wait_event(up[i % 2])
             egrid[i % 2].refresh()
-            batch.score_grid(ubuf[i % 2], egrid[i % 2], TOLS, workspace=ews,
-                             method="bins").cpu()
+            c = batch.score_grid(ubuf[i % 2], egrid[i % 2], TOLS, workspace=ews,
+                                 method="bins")
+            cbuf_h[i % 2].copy_(c, non_blocking=True)   # the step's counts to the host
+            done[i % 2].record(main)
+            if i > 0:
+                done[(i - 1) % 2].synchronize()         # the previous step's counts arrived
+        done[(k - 1) % 2].synchronize()
         e1.record(main)
         e1.synchronize()
         return e0.elapsed_time(e1) / k
 
     e2e_pipelined(2)
-    e2e_ms = e2e_pipelined(max(3, args.steps))
+    e2e_steps = max(3, args.steps)
+    e2e_ms = e2e_pipelined(e2e_steps)
+    e2e_counts_equal = bool(torch.equal(cbuf_h[(e2e_steps - 1) % 2], counts.cpu()))
     e2e_t = torch.tensor([e2e_ms, serial_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
@@ -1199,9 +1210,11 @@ def run_ours(args, rank, world, local_rank):
                 "ms_per_step": float(e2e_t[0].item()),
                 "how": "the timed step's calls (GvecGrid.refresh + score_grid) on inputs "
                        "copied from pinned host memory into the index's g buffer, counts "
-                       "read back to the host, every step; step i+1's copies run on a "
-                       "second stream during step i (two indexes); one timed region over "
-                       "the steps (L2 flushed before each step inside it)",
+                       "read back to the host (pinned) every step; step i+1's copies run "
+                       "on a second stream during step i (two indexes), and the host "
+                       "queues step i+1 before waiting for step i's counts; one timed "
+                       "region over the steps (L2 flushed before each step inside it)",
+                "counts_equal_device_step": e2e_counts_equal,
                 "serial_value": e2e_serial,
                 "serial_how": "a new GvecGrid (bounds read back) + score_grid each step, "
                               "its copies before its compute (CUDA events around each step)"},

@@ -37,6 +37,44 @@ def test_cache_buckets_and_roundtrip(tune, monkeypatch, tmp_path):
     assert tune.score_tile(1000, 5000, 3) == (2, 7)
 
 
+def test_halo_cell_factor(tune):
+    """The smallest cell side with a one-row join halo: W + 2 eps over the
+    default side, W the largest widened box half width of the UBIs the join
+    takes, computed here independently for rotated cubic cells."""
+    import torch
+
+    class Base:
+        cs, gmax, n = 0.03, 1.5, 100000
+
+    rng = np.random.default_rng(3)
+    a = np.array([4.05, 3.0, 5.5])
+    ubis = np.empty((3, 3, 3))
+    for i in range(3):
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        ubis[i] = a[i] * q
+    tol = 0.1
+    G = Base.gmax * (1 + 1e-6)
+    W = 0.0
+    for u in ubis:
+        ub = np.linalg.inv(u)
+        hm = np.ceil(np.abs(u).sum(axis=1) * G + 1.0)
+        w = (tol + 1e-6) * np.linalg.norm(ub, axis=1) * (1 + 1e-9) + \
+            4 * 2.0 ** -24 * hm.max() * np.abs(ub).sum(axis=1)
+        W = max(W, w.max())
+    want = (W + 4e-5 * (1 + G)) * (1 + 1e-3) / Base.cs
+    got = tune.halo_cell_factor(torch.tensor(ubis), Base, tol)
+    assert got == pytest.approx(want, rel=1e-12)
+    assert got == pytest.approx(0.1 / 3.0 / Base.cs, rel=0.01)  # the smallest cell dominates
+    assert tune.halo_cell_factor(torch.tensor(ubis), Base, 0.2) > got
+    # UBIs the join does not take are left out: singular, or more candidate hkl than g
+    big = ubis.copy()
+    big[1] = 0.0
+    big[2] *= 100.0
+    assert tune.halo_cell_factor(torch.tensor(big), Base, tol) == pytest.approx(
+        tune.halo_cell_factor(torch.tensor(ubis[:1]), Base, tol), rel=1e-12)
+    assert tune.halo_cell_factor(torch.tensor(ubis[:0]), Base, tol) is None
+
+
 @pytest.mark.gpu
 def test_every_tile_exact_and_cached(tune, oracle, cuda):
     from imaged11_b200 import batch, synth

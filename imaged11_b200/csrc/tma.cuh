@@ -1,5 +1,5 @@
 // Minimal sm_100a helpers for 1-D TMA bulk copies (global -> shared) completed
-// on an mbarrier, with bounded waits.  No cluster multicast anywhere.
+// on an mbarrier, with bounded waits.  Every copy lands in its own CTA's shared memory.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>

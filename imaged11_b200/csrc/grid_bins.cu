@@ -8,8 +8,9 @@
 // enumerated once per UBI (the lookup scorer's enumeration, its per-candidate
 // work in FP32 with the rounding folded into w) and the boxes are sorted by
 // the row of grid cells holding their centre (fixed y and z cell): counts per
-// row in shared memory per CTA, a scan, and a second enumeration that writes
-// each CTA's boxes of a row as one contiguous run.  One CTA then takes one
+// block of 16 rows in shared memory per CTA, a scan, a second enumeration that
+// writes each CTA's boxes of a block as one sequential stream, and a split of
+// each block into its rows.  One CTA then takes one
 // row: it sorts the row's boxes by x cell in shared memory, stages the
 // g-vectors of the row's region (its y/z cell widened by the largest half
 // width W, all x cells the boxes need) sorted by x cell, and every run of 32
@@ -19,18 +20,19 @@
 // are read by all lanes at once (broadcast) and tested with packed f32x2
 // instructions.
 //
-// Per (box, g), the screening kernel's FP32 arithmetic (score_batch.cu):
-//   h = UBI32 . g32 (FMA chains),  d = h - hkl,  s = d.d;
+// Per (box, g), the screening kernel's FP32 arithmetic (score_batch.cu), with
+// the subtraction of hkl folded into the first FMA of each chain:
+//   d = UBI32 . g32 - hkl (one FMA chain from -hkl),  s = d.d;
 //   s < lo_j           -> counted for tolerance j,
 //   lo_j <= s < hi_j   -> re-evaluated with the reference's exact FP64
 //                         arithmetic, counted when drlv2 < tol_j^2 and the
 //                         rounded h is the box's hkl,
 //   s >= hi_j          -> not counted for j.
-// The band [lo_j, hi_j) is the screening kernel's proven one, from
-// |h32 - h64| <= E = 6 * 2^-24 * S * gmax (S = largest row sum of |UBI|).
-// With every tolerance below 0.4 and S * gmax < 16384 (E < 0.006), a pair
-// with s < hi_j has all |d| < 0.45, so h - hkl is exact in FP32 (Sterbenz),
-// the FP32 value is the screening kernel's, and for s < lo_j the rounded h64
+// The band [lo_j, hi_j) is the screening kernel's proven one with the folded
+// chain's bound |d32 - d64| <= E = 2^-24 * S * (8 gmax + 3 W) (S = largest row
+// sum of |UBI|; partial sums stay below |hkl| + S gmax <= S (2 gmax + W)).
+// With every tolerance below 0.4 and S * gmax < 16384, a pair with s < hi_j
+// has all |d| < 0.5 - E, and for s < lo_j the rounded h64
 // is hkl and drlv2 < tol_j^2: the pair is counted under its own hkl exactly
 // when the reference counts it.  A pair tested against a box of another hkl
 // has some |d| >= 0.5 - E, so s >= 0.2 > hi_j: never counted.  A staged tile
@@ -40,9 +42,14 @@
 // UBIs outside the limits (the lookup plan's caps, hkl beyond -256..255,
 // S * gmax too large) are scored by an exact FP64 scan of every regular g, and
 // the g-vectors outside the regular range by an exact FP64 scan of their list.
-// Counts go to the output with integer atomics (exact); the optional FP64
-// sums of the counted drlv2 are added with double atomics, so their last bits
-// depend on the order the warps finish in.
+// Counts go to the output with integer atomics (exact); the optional sums of
+// the counted drlv2 are added in fixed point (each term rounded to one step,
+// then integer atomics), so they repeat bit for bit.
+//
+// The same pipeline serves the batched assignment (score_and_assign over many
+// grains, k_assign's two passes in gvec_grid.cu): the join's AS modes send
+// every pair the screen cannot exclude from tol^2 to the exact FP64 path and
+// apply the assignment's atomic minima there.
 #include <math.h>
 #include <string.h>
 #include <algorithm>

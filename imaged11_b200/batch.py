@@ -367,9 +367,11 @@ def score_and_assign_grid(ubis, grid, tol, drlv2, labels, grain_labels=None, npk
         if not (float(tol) < BINS_TOL_LIMIT and bins_fit(grid)):
             raise ValueError("method='bins' needs tol < %g and a grid within the join's "
                              "limits" % BINS_TOL_LIMIT)
-        boxes = bins_box_estimate(u, grid, float(tol))
-        bws = workspace if workspace is not None and workspace.fits(m, grid, boxes) else \
-            BinsWorkspace(m, grid, boxes)
+        # a caller's workspace of this shape is used whatever it holds (the
+        # grains then run in ranges of boxes that fit), as in score_grid
+        bws = workspace if isinstance(workspace, BinsWorkspace) and workspace.m >= m and \
+            (workspace.nx, workspace.xsub) == (grid.nx, grid.xsub) else \
+            BinsWorkspace(m, grid, bins_box_estimate(u, grid, float(tol)))
         best = torch.empty(grid.n, dtype=torch.int64, device=dev)
         win = torch.empty(grid.n, dtype=torch.int32, device=dev)
         args = (u.data_ptr(), m)

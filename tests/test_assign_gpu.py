@@ -68,6 +68,32 @@ def test_ties_labels_and_resets(scene, oracle, method, cuda):
     assert np.array_equal(d, ref_d)
 
 
+def test_bins_workspace_ranges(scene, oracle, cuda):
+    """The binned assignment with a workspace holding part of the boxes: the
+    grains run in ranges, each range's boxes rebuilt for the second pass after
+    the first pass has seen every range; too small for one grain's boxes is an
+    error."""
+    from imaged11_b200 import batch
+    from imaged11_b200._lib import ID11BError
+    ps, ubis = scene
+    u = ubis[:120]
+    n = len(ps.gv)
+    d0 = np.zeros(n) + 2
+    l0 = np.zeros(n, np.int32) - 1
+    ref_d, ref_l = sequential(oracle, u, ps.gv, 0.1, d0, l0, range(len(u)))
+    grid = batch.GvecGrid(ps.gv)
+    est = batch.bins_box_estimate(u, grid, 0.1)
+    for frac in (0.5, 0.13):
+        ws = batch.BinsWorkspace(len(u), grid, int(est * frac))
+        d, lab = d0.copy(), l0.copy()
+        batch.score_and_assign_grid(u, grid, 0.1, d, lab, method="bins", workspace=ws)
+        assert np.array_equal(lab, ref_l), frac
+        assert np.array_equal(d, ref_d), frac
+    with pytest.raises(ID11BError):
+        batch.score_and_assign_grid(u, grid, 0.1, d0.copy(), l0.copy(), method="bins",
+                                    workspace=batch.BinsWorkspace(len(u), grid, 10))
+
+
 @pytest.mark.parametrize("method", METHODS)
 def test_special_g_and_device_tensors(golden, oracle, method, cuda):
     import torch
